@@ -1,0 +1,297 @@
+"""ctypes binding of libbsar.so (the C ABI declared in include/bsar.h).
+
+This is the Python-side caller of the drop-in boundary: every method maps to one
+``extern "C"`` entry point and raises :class:`BsarError` with the library's message when
+the call does not return ``BSAR_OK``.  The library must exist; there is no fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent.parent          # c-_bistatic_sar_b200/
+LIB_PATH = PKG / "lib" / "libbsar.so"
+CSRC = PKG / "csrc"
+
+_d = C.POINTER(C.c_double)
+_i64 = C.c_int64
+_i32 = C.c_int32
+
+STATUS = {0: "ok", 1: "invalid argument", 2: "HBM budget exceeded", 3: "device wait timed out",
+          4: "CUDA error", 5: "not found", 6: "unsupported", 7: "queue full"}
+SOLVER = {"grid": 0, "newton": 1}
+LEGS = {"mean": 0, "per_pulse": 1}
+PRECISION = {"fp64": 0, "mixed": 1, "mixed_fp16": 2}
+
+
+class BsarError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class Dem(C.Structure):
+    _fields_ = [("nx", _i64), ("ny", _i64), ("x_vec", _d), ("y_vec", _d), ("z", _d)]
+
+
+class FermatOpts(C.Structure):
+    _fields_ = [("solver", _i32), ("precision", _i32), ("search_radius_m", C.c_double)]
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [("dem", Dem), ("n_pulses", _i64), ("tx", _d), ("rx", _d), ("n_samples", _i64),
+                ("samples", _d), ("samples_kind", _i32), ("upsample", _i32),
+                ("n1", C.c_double), ("n2", C.c_double), ("c", C.c_double), ("fc", C.c_double),
+                ("fs", C.c_double), ("chirp_f0", C.c_double), ("chirp_f1", C.c_double),
+                ("chirp_T", C.c_double)]
+
+
+class Grid(C.Structure):
+    _fields_ = [("nx", _i64), ("ny", _i64), ("nz", _i64), ("x_axis", _d), ("y_axis", _d), ("z_axis", _d)]
+
+
+class BpOpts(C.Structure):
+    _fields_ = [("solver", _i32), ("legs", _i32), ("precision", _i32), ("flags", _i32),
+                ("search_radius_m", C.c_double)]
+
+
+class Opts(C.Structure):
+    _fields_ = [("device", _i32), ("flags", _i32), ("hbm_budget_bytes", C.c_uint64)]
+
+
+def build(quiet: bool = True) -> Path:
+    """Compile libbsar.so for sm_100a (nvcc cross-compiles; no GPU needed)."""
+    out = subprocess.run(["make", "-C", str(CSRC), "-j4"], capture_output=quiet, text=True)
+    if out.returncode != 0:
+        raise RuntimeError(f"libbsar build failed:\n{out.stdout}\n{out.stderr}")
+    return LIB_PATH
+
+
+_LIB = None
+
+
+def lib() -> C.CDLL:
+    """Load libbsar.so (raises when it has not been built)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not LIB_PATH.exists():
+        raise FileNotFoundError(f"{LIB_PATH} is missing: build it with bsar.native.build()")
+    L = C.CDLL(str(LIB_PATH))
+    V = C.c_void_p
+    sigs = {
+        "bsar_create": ([C.POINTER(V), C.POINTER(Opts)], _i32),
+        "bsar_destroy": ([V], None),
+        "bsar_status_string": ([_i32], C.c_char_p),
+        "bsar_last_error": ([V], C.c_char_p),
+        "bsar_set_stream": ([V, V], _i32),
+        "bsar_synchronize": ([V], _i32),
+        "bsar_launch_count": ([V], C.c_uint64),
+        "bsar_bytes_in_use": ([V], C.c_uint64),
+        "bsar_dem_elevation": ([V, C.POINTER(Dem), _d, _i64, _d], _i32),
+        "bsar_refraction_points": ([V, C.POINTER(Dem), _d, _d, _i64, C.c_double, C.c_double,
+                                    C.POINTER(FermatOpts), _d], _i32),
+        "bsar_slant_range_fermat": ([V, C.POINTER(Dem), _d, _d, _i64, _d, C.c_double, C.c_double,
+                                     C.POINTER(FermatOpts), _d, _d, _d, _d], _i32),
+        "bsar_spline_upsample": ([V, _d, _i64, _i64, _i32, _d], _i32),
+        "bsar_fft": ([V, _d, _i64, _i64, _i32], _i32),
+        "bsar_fft_correlate": ([V, _d, _i64, _i64, _d, _i64, _i32, _d], _i32),
+        "bsar_scene_upload": ([V, C.POINTER(SceneDesc), C.POINTER(C.c_uint64)], _i32),
+        "bsar_scene_release": ([V, C.c_uint64], _i32),
+        "bsar_scene_compress": ([V, C.c_uint64, _i32], _i32),
+        "bsar_scene_read_upsampled": ([V, C.c_uint64, _d], _i32),
+        "bsar_backproject": ([V, C.c_uint64, C.POINTER(Grid), C.POINTER(BpOpts), _d], _i32),
+        "bsar_backproject_device": ([V, C.c_uint64, C.POINTER(Grid), C.POINTER(BpOpts), V], _i32),
+    }
+    for name, (args, res) in sigs.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    _LIB = L
+    return L
+
+
+def _f64(a, shape=None):
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+    return a.reshape(shape) if shape is not None else a
+
+
+def _c128(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.complex128))
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(_d)
+
+
+class DemArrays:
+    """Keeps the numpy arrays of a DEM alive next to its C struct."""
+
+    def __init__(self, x_vec, y_vec, z):
+        self.x = _f64(x_vec)
+        self.y = _f64(y_vec)
+        n = len(self.x) * len(self.y)
+        self.z = _f64(z).reshape(-1)[:n] if n else np.zeros(1)
+        self.c = Dem(len(self.x), len(self.y), _p(self.x), _p(self.y), _p(self.z))
+
+
+class Context:
+    """One bsar_ctx on a CUDA device."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0):
+        self.L = lib()
+        h = C.c_void_p()
+        st = self.L.bsar_create(C.byref(h), C.byref(Opts(device, 0, hbm_budget_bytes)))
+        if st != 0:
+            raise BsarError(st, "bsar_create failed (no usable CUDA device?)")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.bsar_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _ok(self, st):
+        if st != 0:
+            raise BsarError(st, self.L.bsar_last_error(self.h).decode())
+
+    # -- context ------------------------------------------------------------------------
+    def set_stream(self, stream_handle: int | None):
+        self._ok(self.L.bsar_set_stream(self.h, C.c_void_p(stream_handle or 0)))
+
+    def synchronize(self):
+        self._ok(self.L.bsar_synchronize(self.h))
+
+    @property
+    def launches(self) -> int:
+        return int(self.L.bsar_launch_count(self.h))
+
+    @property
+    def bytes_in_use(self) -> int:
+        return int(self.L.bsar_bytes_in_use(self.h))
+
+    def last_error(self) -> str:
+        return self.L.bsar_last_error(self.h).decode()
+
+    # -- functional entry points -------------------------------------------------------
+    def dem_elevation(self, dem: DemArrays, xy):
+        xy = _f64(xy, (-1, 2))
+        out = np.empty(len(xy))
+        self._ok(self.L.bsar_dem_elevation(self.h, C.byref(dem.c), _p(xy), len(xy), _p(out)))
+        return out
+
+    def refraction_points(self, dem: DemArrays, p1, p2, n1, n2, solver="grid", search_radius_m=0.0):
+        p1 = _f64(p1, (-1, 3))
+        p2 = _f64(p2, (-1, 3))
+        out = np.empty((len(p1), 3))
+        fo = FermatOpts(SOLVER[solver], 0, search_radius_m)
+        self._ok(self.L.bsar_refraction_points(self.h, C.byref(dem.c), _p(p1), _p(p2), len(p1), n1, n2,
+                                               C.byref(fo), _p(out)))
+        return out
+
+    def slant_range_fermat(self, dem: DemArrays, tx, rx, P, n1, n2, solver="grid", reflection=False,
+                           search_radius_m=0.0):
+        tx = _f64(tx, (-1, 3))
+        rx = _f64(rx, (-1, 3))
+        P = _f64(P, (3,))
+        n = len(tx)
+        ranges = np.empty((4, n))
+        ida = np.empty((n, 3))
+        volta = np.empty((n, 3))
+        refl = np.empty((n, 3)) if reflection else None
+        fo = FermatOpts(SOLVER[solver], 0, search_radius_m)
+        self._ok(self.L.bsar_slant_range_fermat(self.h, C.byref(dem.c), _p(tx), _p(rx), n, _p(P), n1, n2,
+                                                C.byref(fo), _p(ranges), _p(ida), _p(volta), _p(refl)))
+        return ranges, ida, volta, refl
+
+    def spline_upsample(self, data, factor=4):
+        data = _c128(np.atleast_2d(data))
+        b, n = data.shape
+        out = np.empty((b, n * factor), dtype=np.complex128)
+        self._ok(self.L.bsar_spline_upsample(self.h, _p(data.view(np.float64)), n, b, factor,
+                                             _p(out.view(np.float64))))
+        return out
+
+    def fft(self, data, inverse=False):
+        a = np.array(np.atleast_2d(data), dtype=np.complex128, copy=True, order="C")
+        b, n = a.shape
+        self._ok(self.L.bsar_fft(self.h, _p(a.view(np.float64)), n, b, 1 if inverse else 0))
+        return a
+
+    def fft_correlate(self, signal, reference, conj=True):
+        s = _c128(np.atleast_2d(signal))
+        r = _c128(reference)
+        b, ns = s.shape
+        N = max(ns, len(r))
+        out = np.empty((b, N), dtype=np.complex128)
+        self._ok(self.L.bsar_fft_correlate(self.h, _p(s.view(np.float64)), ns, b, _p(r.view(np.float64)),
+                                           len(r), 1 if conj else 0, _p(out.view(np.float64))))
+        return out
+
+    # -- scenes ----------------------------------------------------------------------
+    def scene_upload(self, dem: DemArrays, tx, rx, samples, *, kind="raw", upsample=4, n1=1.0, n2=2.0,
+                     c=3e8, fc=1e9, fs=1.2e9, chirp_f0=0.0, chirp_f1=0.0, chirp_T=0.0) -> int:
+        tx = _f64(tx, (-1, 3))
+        rx = _f64(rx, (-1, 3))
+        smp = _c128(samples)
+        desc = SceneDesc(dem.c, len(tx), _p(tx), _p(rx), smp.shape[1], _p(smp.view(np.float64)),
+                         0 if kind == "raw" else 1, upsample, n1, n2, c, fc, fs, chirp_f0, chirp_f1, chirp_T)
+        sid = C.c_uint64()
+        self._ok(self.L.bsar_scene_upload(self.h, C.byref(desc), C.byref(sid)))
+        return int(sid.value)
+
+    def scene_release(self, sid: int):
+        self._ok(self.L.bsar_scene_release(self.h, sid))
+
+    def scene_compress(self, sid: int, precision="fp64"):
+        self._ok(self.L.bsar_scene_compress(self.h, sid, PRECISION[precision]))
+
+    def scene_read_upsampled(self, sid: int, n_pulses: int, n_out: int):
+        out = np.empty((n_pulses, n_out), dtype=np.complex128)
+        self._ok(self.L.bsar_scene_read_upsampled(self.h, sid, _p(out.view(np.float64))))
+        return out
+
+    @staticmethod
+    def _grid(gx, gy, gz):
+        gx, gy, gz = _f64(gx), _f64(gy), _f64(gz)
+        return (gx, gy, gz), Grid(len(gx), len(gy), len(gz), _p(gx), _p(gy), _p(gz))
+
+    def backproject(self, sid: int, gx, gy, gz, *, solver="grid", legs="mean", precision="fp64",
+                    search_radius_m=0.0):
+        keep, g = self._grid(gx, gy, gz)
+        o = BpOpts(SOLVER[solver], LEGS[legs], PRECISION[precision], 0, search_radius_m)
+        out = np.empty((g.nx, g.ny, g.nz), dtype=np.complex128)
+        self._ok(self.L.bsar_backproject(self.h, sid, C.byref(g), C.byref(o), _p(out.view(np.float64))))
+        return out
+
+    def backproject_device(self, sid: int, gx, gy, gz, d_image_ptr: int, *, solver="grid", legs="mean",
+                           precision="fp64", search_radius_m=0.0):
+        keep, g = self._grid(gx, gy, gz)
+        o = BpOpts(SOLVER[solver], LEGS[legs], PRECISION[precision], 0, search_radius_m)
+        self._ok(self.L.bsar_backproject_device(self.h, sid, C.byref(g), C.byref(o), C.c_void_p(d_image_ptr)))
+
+
+def upload_scene(ctx: Context, scene, kind="raw") -> int:
+    """Upload a bsar.scene.Scene (raw echoes) to the context."""
+    sp = scene.spec
+    dem = DemArrays(scene.x_vec, scene.y_vec, scene.z)
+    f0, f1 = -sp.bandwidth / 2.0, sp.bandwidth / 2.0
+    return ctx.scene_upload(dem, scene.tx, scene.rx, scene.raw, kind=kind, upsample=sp.upsample,
+                            n1=sp.n1, n2=sp.n2, c=3e8, fc=sp.fc, fs=sp.fs, chirp_f0=f0, chirp_f1=f1,
+                            chirp_T=sp.pulse_T)

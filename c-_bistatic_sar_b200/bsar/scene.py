@@ -320,11 +320,11 @@ def fermat_newton(x_vec, y_vec, z, A, B, na, nb, search_nodes=None):
             bestL = np.where(m, Lv, bestL)
             bi = np.where(m, iic, bi)
             bj = np.where(m, jjc, bj)
+    bfi = np.minimum(bi, nxd - 2)
+    bfj = np.minimum(bj, nyd - 2)
     bestF = np.full(len(A), np.inf)
-    bu = np.zeros(len(A))
-    bv = np.zeros(len(A))
-    bfi = np.zeros(len(A), np.int64)
-    bfj = np.zeros(len(A), np.int64)
+    bu = (bi - bfi).astype(np.float64)
+    bv = (bj - bfj).astype(np.float64)
     for k in range(4):
         fi = bi - 1 + (k >> 1)
         fj = bj - 1 + (k & 1)

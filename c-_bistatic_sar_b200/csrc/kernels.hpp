@@ -1,0 +1,80 @@
+// kernels.hpp -- launch interface between the host runtime (bsar_api.cpp) and the
+// CUDA translation units.  Plain structs of device pointers and sizes.
+#pragma once
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "dev_view.hpp"
+
+namespace bsar {
+
+// ------------------------------- pulse / FFT ----------------------------------------
+struct PulseArgs {
+    const double2* in;   // batch x ns raw samples (complex128)
+    int64_t batch;
+    int ns;
+    int P, logP;         // padded FFT length
+    const void* tw;      // P/2 twiddles, real_bytes precision
+    const void* spec;    // P reference-spectrum entries, bit-reversed order
+    int real_bytes;      // 8: FP64 transform, 4: FP32 transform
+    int n_keep;          // compressed samples kept per pulse
+    int factor;          // 0: keep compressed (complex128 -> out64); >0 upsample
+    int out_kind;        // 0 complex128, 1 complex64, 2 FP16 complex + per-pulse scale
+    double2* out64;
+    float2* out32;
+    __half2* out16;
+    float* scale16;
+};
+
+cudaError_t launch_ref_spectrum(const double2* ref, int nref, int P, int logP, const void* tw, int correlate,
+                                void* spec, int real_bytes, cudaStream_t st);
+cudaError_t launch_pulse_compress(const PulseArgs& a, cudaStream_t st);
+cudaError_t launch_fft_rows(double2* data, int64_t batch, int P, int logP, const double2* tw, int inverse,
+                            cudaStream_t st);
+cudaError_t launch_spline(const double2* in, int64_t n, int64_t batch, int factor, double2* out,
+                          cudaStream_t st);
+
+// ------------------------------- Fermat (FP64) ---------------------------------------
+cudaError_t launch_dem_elevation(const DemView& d, const double* xy, int64_t n, double* z, cudaStream_t st);
+cudaError_t launch_refraction_points(const DemView& d, const double* p1, const double* p2, int64_t n, double n1,
+                                     double n2, int solver, int W, double* out, cudaStream_t st);
+cudaError_t launch_slant_range(const DemView& d, const double* tx, const double* rx, int64_t np,
+                               const double* target, double n1, double n2, int solver, int W, double* ranges,
+                               double* ida, double* volta, double* refl, cudaStream_t st);
+
+// ------------------------------- back-projection -------------------------------------
+struct BpArgs {
+    DemView dem;
+    const double* tx;     // np x 3
+    const double* rx;     // np x 3
+    int np;
+    int64_t nr;           // upsampled samples per pulse
+    const double2* rc64;  // np x nr (FP64 form)
+    const float2* rc32;   // np x nr (mixed)
+    const __half2* rc16;  // np x nr (mixed FP16)
+    const float* scale16; // np per-pulse scales (mixed FP16)
+    const double* gx;
+    const double* gy;
+    const double* gz;
+    int nx, ny, nz;
+    double n1, n2, c, fs_eff, lambda;
+    int W;                // Newton node-scan half width
+    int64_t v_begin, v_count;  // voxel range, reference flat order (z -> x -> y)
+    double2* out;         // image [x][y][z]
+    // mixed form: per-pulse FP64 reference optical path and reduced carrier phase
+    const double* ref_L;    // np
+    const float* ref_phase; // np, (2 pi / lambda) * ref_L reduced to [-pi, pi)
+    const int* ref_bin_i;   // np, floor(ref_L * fs_eff / c)
+    const float* ref_bin_f; // np, ref_L * fs_eff / c - ref_bin_i
+};
+
+cudaError_t launch_bp_plain(const BpArgs& a, int solver, int legs, cudaStream_t st);
+cudaError_t launch_bp_mixed(const BpArgs& a, int legs, int fp16, cudaStream_t st);
+cudaError_t launch_ref_ranges(const DemView& d, const double* tx, const double* rx, int np, const double* center,
+                              double n1, double n2, int W, double lambda, double bin_per_m, double* ref_L,
+                              float* ref_phase, int* ref_bin_i, float* ref_bin_f, cudaStream_t st);
+
+}  // namespace bsar

@@ -1,0 +1,218 @@
+/*
+ * bsar.h -- C ABI of the B200 bistatic SAR back-projection library (libbsar.so).
+ *
+ * Drop-in boundary for the hot path of DavidAtenciaMondragon/c-_bistatic_sar:
+ * pulse compression (fft_utils) -> x4 Hermite fast-time upsampling (interpolation)
+ * -> Fermat refraction solve (raw_data_processing) -> back-projection (the voxel
+ * loop inline in proc_test_script.cpp).  Each entry point below names the reference
+ * function or code block it replaces (path:line inside the reference project).
+ *
+ * Conventions
+ *   - Plain pointers and sizes only.  Complex arrays are interleaved (re, im) double
+ *     pairs; point arrays are n x 3 row-major (x, y, z); pulses are pulse-major
+ *     (sample s of pulse p at [p * n + s]).
+ *   - Host buffers are caller-owned and only read / written during the call; device
+ *     memory is owned by the context.  Every call is synchronous unless its name ends
+ *     in _device.
+ *   - Every entry point returns a bsar_status; bsar_last_error() gives the message.
+ *     There is no CPU fallback: without a usable CUDA device bsar_create fails.
+ *   - A context is internally locked; calls from several threads are serialised.
+ */
+#ifndef BSAR_H
+#define BSAR_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BSAR_ABI_VERSION 1
+
+typedef enum bsar_status {
+    BSAR_OK = 0,
+    BSAR_ERR_INVALID_ARG = 1,  /* malformed sizes, null pointers, non-finite geometry */
+    BSAR_ERR_OOM_BUDGET = 2,   /* the request does not fit the context's HBM budget  */
+    BSAR_ERR_TIMEOUT = 3,      /* a bounded device-side wait ran out                 */
+    BSAR_ERR_CUDA = 4,         /* a CUDA runtime error (message in bsar_last_error)  */
+    BSAR_ERR_NOT_FOUND = 5,    /* unknown scene or request id                        */
+    BSAR_ERR_UNSUPPORTED = 6,  /* a valid request outside what this build implements */
+    BSAR_ERR_QUEUE_FULL = 7    /* serving: no admission slot right now               */
+} bsar_status;
+
+/* Fermat crossing-point solver. */
+typedef enum bsar_solver {
+    BSAR_SOLVER_GRID = 0,   /* the reference's 5-level 709-point grid search,
+                               src/raw_data_processing.cpp:455-572 (bit-exact in FP64) */
+    BSAR_SOLVER_NEWTON = 1  /* node scan + Newton on the bilinear DEM facets           */
+} bsar_solver;
+
+/* Leg distances R1t / R1r used by back-projection. */
+typedef enum bsar_legs {
+    BSAR_LEGS_MEAN = 0,      /* mean over all pulses, as shipped (proc_test_script.cpp:518-548) */
+    BSAR_LEGS_PER_PULSE = 1  /* r1Tx / r1Rx of the pulse itself (src/raw_data_processing.cpp:197-215) */
+} bsar_legs;
+
+typedef enum bsar_precision {
+    BSAR_FP64 = 0,        /* plain: FP64 delays, FP64 complex samples and sums            */
+    BSAR_MIXED = 1,       /* FP32 differential delays vs an FP64 per-pulse reference range,
+                             complex64 samples, Kahan-compensated FP32 sums               */
+    BSAR_MIXED_FP16 = 2   /* as MIXED, samples stored FP16 complex with an FP32 pulse scale */
+} bsar_precision;
+
+typedef struct bsar_ctx bsar_ctx;
+typedef uint64_t bsar_scene_id;
+
+typedef struct bsar_opts {
+    int32_t device;             /* CUDA device ordinal                                  */
+    int32_t flags;              /* reserved, must be 0                                  */
+    uint64_t hbm_budget_bytes;  /* device bytes the context may hold; 0 = 90 % of free */
+} bsar_opts;
+
+/* ProcessedDEM (reference include/radar_params.h:75-79): X_vec, Y_vec, Z_DEM[y][x].
+ * nx == 0 or ny == 0 is an empty DEM (flat surface z = 0, src/raw_data_processing.cpp:616-618).
+ * z holds ny * nx heights, z[j * nx + i] = Z_DEM[j][i]; pack a ragged Z_DEM with 0.0
+ * where the reference would find no entry (:649-652). */
+typedef struct bsar_dem {
+    int64_t nx, ny;
+    const double* x_vec;
+    const double* y_vec;
+    const double* z;
+} bsar_dem;
+
+typedef struct bsar_fermat_opts {
+    int32_t solver;          /* bsar_solver                                                */
+    int32_t precision;       /* BSAR_FP64, or BSAR_MIXED (FP32 scan + FP64 final step)     */
+    double search_radius_m;  /* Newton node-scan radius around the flat-interface start;
+                                <= 0 selects 1.5 m                                         */
+} bsar_fermat_opts;
+
+/* ---------------------------------------------------------------------------------
+ * Context
+ * ------------------------------------------------------------------------------- */
+bsar_status bsar_create(bsar_ctx** out, const bsar_opts* opts);
+void bsar_destroy(bsar_ctx* ctx);
+const char* bsar_status_string(bsar_status status);
+const char* bsar_last_error(const bsar_ctx* ctx);
+/* Use a caller-owned cudaStream_t for all work of this context (NULL = own stream). */
+bsar_status bsar_set_stream(bsar_ctx* ctx, void* cuda_stream);
+bsar_status bsar_synchronize(bsar_ctx* ctx);
+/* Number of this library's kernel launches issued by the context so far. */
+uint64_t bsar_launch_count(const bsar_ctx* ctx);
+/* Device bytes currently held by the context (scenes, work buffers). */
+uint64_t bsar_bytes_in_use(const bsar_ctx* ctx);
+
+/* ---------------------------------------------------------------------------------
+ * Functional entry points: the reference functions, batched.
+ * ------------------------------------------------------------------------------- */
+
+/* interpolateDEMElevation, src/raw_data_processing.cpp:615-680, for n points (x, y)
+ * (xy: n x 2) -> z_out[n].  Bit-exact with the reference. */
+bsar_status bsar_dem_elevation(bsar_ctx* ctx, const bsar_dem* dem, const double* xy, int64_t n,
+                               double* z_out);
+
+/* calculateRefractionPoint, src/raw_data_processing.cpp:455-572, for n (start, end)
+ * pairs (n x 3 each) with indices n1 (start side) and n2 (end side) -> points_out (n x 3). */
+bsar_status bsar_refraction_points(bsar_ctx* ctx, const bsar_dem* dem, const double* p_start,
+                                   const double* p_end, int64_t n, double n1, double n2,
+                                   const bsar_fermat_opts* fopts, double* points_out);
+
+/* calculaSlantRangeFermat, src/raw_data_processing.cpp:112-255, for one target over
+ * n_pulses Tx/Rx positions (n x 3).  ranges: 4 x n (r1Tx, r2Tx, r1Rx, r2Rx); refr_ida /
+ * refr_volta: n x 3; reflection (n x 3, may be NULL): calculateReflectionPoint (:575-612). */
+bsar_status bsar_slant_range_fermat(bsar_ctx* ctx, const bsar_dem* dem, const double* tx,
+                                    const double* rx, int64_t n_pulses, const double* target,
+                                    double n1, double n2, const bsar_fermat_opts* fopts,
+                                    double* ranges, double* refr_ida, double* refr_volta,
+                                    double* reflection);
+
+/* splineInterpolation, src/interpolation.cpp:4-51, on `batch` pulses of n complex
+ * samples -> batch x (n * factor).  Bit-exact with the reference; n must be >= 2. */
+bsar_status bsar_spline_upsample(bsar_ctx* ctx, const double* in, int64_t n, int64_t batch,
+                                 int32_t factor, double* out);
+
+/* FFTProcessor::fft / ::ifft, src/fft_utils.cpp:11-61, in place on `batch` rows of n
+ * complex samples.  As in the reference, a row whose length is not a power of two is
+ * left unchanged (the call still returns BSAR_OK and records a message). */
+bsar_status bsar_fft(bsar_ctx* ctx, double* data, int64_t n, int64_t batch, int32_t inverse);
+
+/* FFTProcessor::fftCorrelation (conjugate = 1, src/fft_utils.cpp:63-101) or
+ * ::fftConvolution (conjugate = 0, :103-138) of `batch` rows of n_signal samples against
+ * one reference of n_reference samples; out: batch x max(n_signal, n_reference). */
+bsar_status bsar_fft_correlate(bsar_ctx* ctx, const double* signal, int64_t n_signal,
+                               int64_t batch, const double* reference, int64_t n_reference,
+                               int32_t conjugate, double* out);
+
+/* ---------------------------------------------------------------------------------
+ * Resident scenes: DEM, trajectories and pulses stay in HBM between calls.
+ * ------------------------------------------------------------------------------- */
+typedef enum bsar_samples_kind {
+    BSAR_SAMPLES_RAW = 0,        /* raw echoes: bsar_scene_compress runs pulse compression */
+    BSAR_SAMPLES_COMPRESSED = 1  /* already range-compressed (rootData), not upsampled     */
+} bsar_samples_kind;
+
+typedef struct bsar_scene_desc {
+    bsar_dem dem;
+    int64_t n_pulses;          /* Np */
+    const double* tx;          /* Np x 3 transmitter positions (Tx_positions.csv) */
+    const double* rx;          /* Np x 3 receiver positions    (Rx_positions.csv) */
+    int64_t n_samples;         /* Ns fast-time samples per pulse (a power of two)   */
+    const double* samples;     /* Np x Ns complex, pulse-major                       */
+    int32_t samples_kind;      /* bsar_samples_kind                                 */
+    int32_t upsample;          /* fast-time factor (the reference uses 4,
+                                  proc_test_script.cpp:220)                          */
+    double n1, n2;             /* refractive indices above / below the surface      */
+    double c;                  /* propagation speed (reference: 3e8)                */
+    double fc;                 /* carrier frequency; lambda = c / fc                 */
+    double fs;                 /* raw sampling rate; back-projection uses fs*upsample */
+    double chirp_f0, chirp_f1; /* LFM chirp start / stop frequency (baseband)        */
+    double chirp_T;            /* pulse duration                                    */
+} bsar_scene_desc;
+
+bsar_status bsar_scene_upload(bsar_ctx* ctx, const bsar_scene_desc* desc, bsar_scene_id* out);
+bsar_status bsar_scene_release(bsar_ctx* ctx, bsar_scene_id scene);
+
+/* Pulse compression + upsampling of a resident scene, one launch over all pulses:
+ * rootData = IFFT(FFT(raw) . conj(FFT(reference))) per pulse (processRawData,
+ * src/raw_data_processing.cpp:371-446) followed by the x`upsample` Hermite interpolation
+ * (proc_test_script.cpp:326-350), stored for `precision` (FP64 / complex64 / FP16 +
+ * scale).  For BSAR_SAMPLES_COMPRESSED scenes only the upsampling runs. */
+bsar_status bsar_scene_compress(bsar_ctx* ctx, bsar_scene_id scene, int32_t precision);
+
+/* Copy the scene's upsampled FP64 pulses (Np x Ns*upsample) to the host (diagnostics). */
+bsar_status bsar_scene_read_upsampled(bsar_ctx* ctx, bsar_scene_id scene, double* out);
+
+typedef struct bsar_grid {
+    int64_t nx, ny, nz;
+    const double* x_axis;   /* grid_xAxis */
+    const double* y_axis;   /* grid_yAxis */
+    const double* z_axis;   /* grid_zAxis */
+} bsar_grid;
+
+typedef struct bsar_bp_opts {
+    int32_t solver;          /* bsar_solver    */
+    int32_t legs;            /* bsar_legs      */
+    int32_t precision;       /* bsar_precision */
+    int32_t flags;           /* reserved, 0    */
+    double search_radius_m;  /* Newton node-scan radius (<= 0: 1.5 m) */
+} bsar_bp_opts;
+
+/* The imager's voxel loop, proc_test_script.cpp:451-767: for every voxel the Fermat
+ * solves of all pulses, the delays / phases (:559-577) and the interpolated, phase-
+ * corrected sum (:583-669).  image_out: complex nx x ny x nz, z fastest -- the layout
+ * of output[x][y][z] (:761-767).  Runs bsar_scene_compress first if the scene has not
+ * been compressed for this precision. */
+bsar_status bsar_backproject(bsar_ctx* ctx, bsar_scene_id scene, const bsar_grid* grid,
+                             const bsar_bp_opts* opts, double* image_out);
+
+/* As bsar_backproject, but asynchronous on the context stream with the image written to
+ * device memory d_image (complex128, same layout); the grid axes are read at the call. */
+bsar_status bsar_backproject_device(bsar_ctx* ctx, bsar_scene_id scene, const bsar_grid* grid,
+                                    const bsar_bp_opts* opts, void* d_image);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BSAR_H */

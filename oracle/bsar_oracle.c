@@ -339,8 +339,9 @@ void bo_refraction_newton(double x1, double y1, double z1, double x2, double y2,
             }
         }
     }
-    double bestF = INFINITY, bu = 0.0, bv = 0.0;
-    int64_t bfi = -1, bfj = -1;
+    /* fallback facet (kept only when no facet path compares below +inf, e.g. NaN input) */
+    int64_t bfi = bi < d->nx - 2 ? bi : d->nx - 2, bfj = bj < d->ny - 2 ? bj : d->ny - 2;
+    double bestF = INFINITY, bu = (double)(bi - bfi), bv = (double)(bj - bfj);
     for (int k = 0; k < 4; k++) {
         int64_t fi = bi - 1 + (k >> 1), fj = bj - 1 + (k & 1);
         if (fi < 0 || fj < 0 || fi > d->nx - 2 || fj > d->ny - 2) continue;

@@ -1,0 +1,120 @@
+"""GPU back-projection through the C ABI against the oracle.
+
+* plain FP64 form, grid solver (the reference's algorithm), mean or per-pulse legs:
+  rel-L2 <= 1e-9 and the same argmax voxel as the oracle restatement of
+  proc_test_script.cpp:451-767;
+* plain FP64 Newton form against the oracle's FP64 Newton: rel-L2 <= 1e-9;
+* mixed forms against the plain FP64 Newton image: rel-L2 <= 1e-3, max phase error
+  <= 0.01 rad, same argmax voxel.
+"""
+import numpy as np
+import pytest
+
+import bsar
+from bsar import scene as S
+import oracle as O
+
+from conftest import max_phase_err, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(spec):
+    sc = S.make_scene(spec)
+    return sc
+
+
+@pytest.fixture(scope="module")
+def small():
+    # config-1 geometry, fewer pulses and voxels so the CPU oracle finishes in seconds
+    return _setup(S.scaled(S.config_spec(1), n_pulses=40, nx=9, ny=9, nz=5, dxy=0.16, dz=0.32))
+
+
+@pytest.fixture(scope="module")
+def rough():
+    return _setup(S.scaled(S.config_spec(2), n_pulses=48, n_samples=4096, nx=11, ny=11, nz=6, dxy=0.1, dz=0.1,
+                           n_scatterers=4))
+
+
+def _oracle_image(oracle, sc, legs, solver):
+    sp = sc.spec
+    dem = O.Dem(sc.x_vec, sc.y_vec, sc.z)
+    rc = oracle.spline_upsample(oracle.fft_correlate(sc.raw, sc.reference), sp.upsample)
+    return oracle.backproject(dem, sc.tx, sc.rx, rc, sc.gx, sc.gy, sc.gz, sp.n1, sp.n2, 3e8, sc.fs_eff, sc.lam,
+                              legs="mean" if legs == "mean" else "per", solver=solver,
+                              search_nodes=S.search_nodes_for(sc.x_vec, sc.y_vec))
+
+
+@pytest.mark.parametrize("legs", ["mean", "per_pulse"])
+def test_plain_grid_matches_reference_algorithm(ctx, oracle, small, legs):
+    sid = bsar.upload_scene(ctx, small)
+    try:
+        img = ctx.backproject(sid, small.gx, small.gy, small.gz, solver="grid", legs=legs, precision="fp64")
+    finally:
+        ctx.scene_release(sid)
+    ref = _oracle_image(oracle, small, legs, "grid")
+    assert rel_l2(img, ref) <= 1e-9
+    assert np.argmax(np.abs(img)) == np.argmax(np.abs(ref))
+
+
+@pytest.mark.parametrize("which", ["small", "rough"])
+def test_plain_newton_matches_oracle(ctx, oracle, which, request):
+    sc = request.getfixturevalue(which)
+    sid = bsar.upload_scene(ctx, sc)
+    try:
+        img = ctx.backproject(sid, sc.gx, sc.gy, sc.gz, solver="newton", legs="per_pulse", precision="fp64")
+    finally:
+        ctx.scene_release(sid)
+    ref = _oracle_image(oracle, sc, "per_pulse", "newton")
+    assert rel_l2(img, ref) <= 1e-9
+    assert np.argmax(np.abs(img)) == np.argmax(np.abs(ref))
+
+
+@pytest.mark.parametrize("precision", ["mixed", "mixed_fp16"])
+@pytest.mark.parametrize("which", ["small", "rough"])
+def test_mixed_matches_fp64(ctx, which, precision, request):
+    sc = request.getfixturevalue(which)
+    sid = bsar.upload_scene(ctx, sc)
+    try:
+        ref = ctx.backproject(sid, sc.gx, sc.gy, sc.gz, solver="newton", legs="per_pulse", precision="fp64")
+        img = ctx.backproject(sid, sc.gx, sc.gy, sc.gz, solver="newton", legs="per_pulse", precision=precision)
+    finally:
+        ctx.scene_release(sid)
+    assert rel_l2(img, ref) <= 1e-3
+    assert max_phase_err(img, ref) <= 0.01
+    assert np.argmax(np.abs(img)) == np.argmax(np.abs(ref))
+
+
+def test_scatterer_focuses_at_its_voxel(ctx):
+    spec = S.scaled(S.config_spec(1), n_pulses=64, nx=15, ny=15, nz=9, dxy=0.04, dz=0.08, n_scatterers=1,
+                    snr_db=np.inf)
+    sc = S.make_scene(spec)
+    sid = bsar.upload_scene(ctx, sc)
+    try:
+        img = ctx.backproject(sid, sc.gx, sc.gy, sc.gz, solver="newton", legs="per_pulse", precision="mixed")
+    finally:
+        ctx.scene_release(sid)
+    ix, iy, iz = np.unravel_index(np.argmax(np.abs(img)), img.shape)
+    assert (ix, iy, iz) == tuple(sc.scat_voxel[0])
+
+
+def test_invalid_requests_are_rejected(ctx, small):
+    sid = bsar.upload_scene(ctx, small)
+    try:
+        with pytest.raises(bsar.BsarError) as e:
+            ctx.backproject(sid, small.gx, small.gy, small.gz, solver="grid", legs="per_pulse", precision="mixed")
+        assert e.value.status == 6
+        with pytest.raises(bsar.BsarError) as e:
+            ctx.backproject(sid, [], small.gy, small.gz)
+        assert e.value.status == 1
+    finally:
+        ctx.scene_release(sid)
+    with pytest.raises(bsar.BsarError) as e:
+        ctx.backproject(987654, small.gx, small.gy, small.gz)
+    assert e.value.status == 5
+    tx = small.tx.copy()
+    tx[3, 1] = np.nan
+    with pytest.raises(bsar.BsarError) as e:
+        ctx.scene_upload(bsar.DemArrays(small.x_vec, small.y_vec, small.z), tx, small.rx, small.raw,
+                         chirp_T=1e-6, chirp_f0=-2.5e8, chirp_f1=2.5e8)
+    assert e.value.status == 1

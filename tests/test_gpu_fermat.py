@@ -1,0 +1,77 @@
+"""GPU Fermat and DEM kernels through the C ABI against the oracle (bit-exact in FP64)."""
+import numpy as np
+import pytest
+
+import bsar
+from bsar import scene as S
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def sc1():
+    return S.make_scene(S.scaled(S.config_spec(1), n_pulses=48), with_raw=False)
+
+
+@pytest.fixture(scope="module")
+def sc2():
+    return S.make_scene(S.scaled(S.config_spec(2), n_pulses=48), with_raw=False)
+
+
+def test_dem_elevation_bitexact(ctx, oracle, sc1):
+    rng = np.random.default_rng(11)
+    xy = np.concatenate([rng.uniform(-20, 60, size=(20000, 2)),
+                         np.stack([sc1.x_vec[rng.integers(0, 64, 500)], sc1.y_vec[rng.integers(0, 64, 500)]], 1),
+                         [[np.nan, 1.0], [np.inf, -np.inf]]])
+    g = ctx.dem_elevation(bsar.DemArrays(sc1.x_vec, sc1.y_vec, sc1.z), xy)
+    o = oracle.dem_elevation(O.Dem(sc1.x_vec, sc1.y_vec, sc1.z), xy)
+    assert np.array_equal(g, o, equal_nan=True)
+
+
+def test_dem_elevation_nonmonotonic_and_empty(ctx, oracle):
+    xv, yv = np.array([3.0, 2.0, 2.5, 1.0]), np.array([0.0, 1.0, 1.0, 2.0])
+    z = np.arange(16, dtype=float).reshape(4, 4) * 0.25
+    xy = np.random.default_rng(2).uniform(-1, 4, size=(2000, 2))
+    assert np.array_equal(ctx.dem_elevation(bsar.DemArrays(xv, yv, z), xy), oracle.dem_elevation(O.Dem(xv, yv, z), xy))
+    assert np.all(ctx.dem_elevation(bsar.DemArrays([], [], np.zeros(0)), xy) == 0.0)
+
+
+@pytest.mark.parametrize("which", ["sc1", "sc2"])
+def test_grid_refraction_bitexact(ctx, oracle, which, request):
+    sc = request.getfixturevalue(which)
+    sp = sc.spec
+    rng = np.random.default_rng(5)
+    n = 256
+    P = np.stack([rng.choice(sc.gx, n), rng.choice(sc.gy, n), rng.choice(sc.gz, n)], 1)
+    A = sc.tx[rng.integers(0, len(sc.tx), n)]
+    g = ctx.refraction_points(bsar.DemArrays(sc.x_vec, sc.y_vec, sc.z), A, P, sp.n1, sp.n2, solver="grid")
+    o = oracle.refraction_points(O.Dem(sc.x_vec, sc.y_vec, sc.z), A, P, sp.n1, sp.n2, solver="grid")
+    assert np.array_equal(g, o)
+
+
+@pytest.mark.parametrize("which", ["sc1", "sc2"])
+def test_newton_refraction_bitexact(ctx, oracle, which, request):
+    sc = request.getfixturevalue(which)
+    sp = sc.spec
+    rng = np.random.default_rng(6)
+    n = 2048
+    P = np.stack([rng.choice(sc.gx, n), rng.choice(sc.gy, n), rng.choice(sc.gz, n)], 1)
+    R = sc.rx[rng.integers(0, len(sc.rx), n)]
+    W = S.search_nodes_for(sc.x_vec, sc.y_vec)
+    g = ctx.refraction_points(bsar.DemArrays(sc.x_vec, sc.y_vec, sc.z), P, R, sp.n2, sp.n1, solver="newton")
+    o = oracle.refraction_points(O.Dem(sc.x_vec, sc.y_vec, sc.z), P, R, sp.n2, sp.n1, solver="newton", search_nodes=W)
+    assert np.array_equal(g, o)
+
+
+@pytest.mark.parametrize("solver", ["grid", "newton"])
+def test_slant_range_fermat_bitexact(ctx, oracle, sc1, solver):
+    sp = sc1.spec
+    W = S.search_nodes_for(sc1.x_vec, sc1.y_vec)
+    P = [20.04, -0.12, -4.9]
+    g = ctx.slant_range_fermat(bsar.DemArrays(sc1.x_vec, sc1.y_vec, sc1.z), sc1.tx, sc1.rx, P, sp.n1, sp.n2,
+                               solver=solver, reflection=True)
+    o = oracle.slant_range_fermat(O.Dem(sc1.x_vec, sc1.y_vec, sc1.z), sc1.tx, sc1.rx, P, sp.n1, sp.n2,
+                                  solver=solver, reflection=True, search_nodes=W)
+    for a, b in zip(g, o):
+        assert np.array_equal(a, b)
