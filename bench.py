@@ -1,0 +1,425 @@
+"""Benchmark: bistatic SAR back-projection, voxel-pulses per second (Fermat included).
+
+Workload: the medium scene (161 x 161 x 81 voxels at 0.02 m centred 20 m downrange and
+5 m deep, 1024 pulses, 8192 fast-time samples x4 upsampled, 256 x 256 fBm DEM at
+0.25 m with sigma 0.3 m, eps_r 6, 50 scatterers, 15 dB SNR; seeded synthetic data).
+
+One step = the whole hot path on one batch: pulse compression + x4 upsampling of all
+pulses (one launch) and the back-projection of every voxel with both Fermat solves of
+every pulse (one launch), image left in HBM.
+
+  value   mixed form (FP32 Newton scan/polish + FP64 final step, FP32 differential
+          delays, complex64 samples, Kahan sums) with the raw pulses resident in HBM
+  e2e     the same through the C ABI with host buffers: scene upload from pinned host
+          memory, compression, back-projection and the image read back every step
+  forms   the plain FP64 Newton form (the >= 2x comparator), the FP16-sample mixed form,
+          and the reference's own algorithm (grid search, mean legs) in FP64 on the GPU
+          over a voxel subset, with the accuracy of the mixed image against FP64
+
+--impl reference times the reference's CPU implementation (its own sources compiled
+under oracle/_ref, OpenMP over the host cores) on a bounded voxel sample of the same
+scene.  Multi-GPU (torchrun): every rank images its own z-slab of the same size (weak
+scaling, no collective in the data path); timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "c-_bistatic_sar_b200"))
+
+METRIC = "BP voxel-pulses/s (Fermat incl.), mixed vs FP64 @<=1e-3 rel-L2; served p99 ms"
+UNIT = "voxel-pulses/s"
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d, "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (SM clock, throttle reasons)."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.thread.join(timeout=2)
+
+    def summary(self):
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows if len(r) >= 9 for k in range(4)
+                          if r[5 + k].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(sm)}
+
+
+# ------------------------------------------------------------------------------------
+def fp32_flops_per_voxel_pulse(W: int) -> int:
+    """Algorithmic FP32 work of the mixed kernel per voxel-pulse (FMA = 2 flops), counted
+    from k_mixed.cu: per Fermat solve a (2W+1)^2 node scan at 17 flops per node, 4 facets x
+    3 polish steps at 80 flops and 4 facet evaluations at 25, a 4-step flat start at 19
+    flops (+ 20 setup); two solves per voxel-pulse plus 40 flops of delay / phase /
+    interpolation / Kahan work."""
+    per_solve = (2 * W + 1) ** 2 * 17 + 4 * 3 * 80 + 4 * 25 + 4 * 19 + 20
+    return 2 * per_solve + 40
+
+
+def sfu_ops_per_voxel_pulse(W: int) -> int:
+    """MUFU operations per voxel-pulse: 2 rsqrt per scanned node, 4 per polish step
+    (2 rsqrt + 2 rcp), 2 per facet evaluation, 2 per flat step; sincos = 2."""
+    per_solve = (2 * W + 1) ** 2 * 2 + 4 * 3 * 4 + 4 * 2 + 4 * 2
+    return 2 * per_solve + 2
+
+
+def make_workload(cfg: int, rank: int):
+    from bsar import scene as S
+
+    spec = S.config_spec(cfg)
+    sc = S.make_scene(spec)
+    if rank:
+        # weak scaling: rank r images the next z-slab of the same size
+        sc.gz = sc.gz - rank * spec.nz * spec.dz
+    return sc
+
+
+def time_device(ctx, torch, stream, sid, sc, precision, solver, legs, steps, warmup, gx=None, gy=None, gz=None):
+    """Device time of `steps` steps (compression + back-projection), CUDA events on the
+    library's stream; also the back-projection kernel alone."""
+    gx = sc.gx if gx is None else gx
+    gy = sc.gy if gy is None else gy
+    gz = sc.gz if gz is None else gz
+    nv = len(gx) * len(gy) * len(gz)
+    img = torch.empty((nv, 2), dtype=torch.float64, device="cuda")
+    ptr = img.data_ptr()
+
+    def step(ev=None):
+        ctx.scene_compress(sid, precision)
+        if ev is not None:
+            ev[0].record(stream)
+        ctx.backproject_device(sid, gx, gy, gz, ptr, solver=solver, legs=legs, precision=precision)
+        if ev is not None:
+            ev[1].record(stream)
+
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    launches0 = ctx.launches
+    t0.record(stream)
+    for k in range(steps):
+        step(kev[k])
+    t1.record(stream)
+    torch.cuda.synchronize()
+    total_ms = t0.elapsed_time(t1)
+    bp_ms = [a.elapsed_time(b) for a, b in kev]
+    return total_ms, bp_ms, img, ctx.launches - launches0
+
+
+def cpu_reference_rate(sc, seconds: float, threads: int, use_ref: bool = True):
+    """Reference CPU path (grid search, mean legs) on a bounded voxel sample.
+    Returns (voxel-pulses/s for a full image, details)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+
+    kind = "reference" if (use_ref and O.Reference.available()) else "port"
+    impl = O.Reference() if kind == "reference" else O.Oracle()
+    sp = sc.spec
+    dem = O.Dem(sc.x_vec, sc.y_vec, sc.z)
+    # pulse compression + upsampling of every pulse (processRawData / splineInterpolation)
+    t = time.perf_counter()
+    rc = impl.fft_correlate(sc.raw, sc.reference)
+    t_pc = time.perf_counter() - t
+    t = time.perf_counter()
+    rc = impl.spline_upsample(rc, sp.upsample)
+    t_up = time.perf_counter() - t
+    nv_total = sp.nx * sp.ny * sp.nz
+    rng = np.random.default_rng(0x5A4B0002)
+    kw = dict(legs="mean")
+    if kind == "reference":
+        kw["nthreads"] = threads
+    else:
+        kw["solver"] = "grid"
+
+    def run(n):
+        vox = rng.choice(nv_total, size=n, replace=False)
+        t0 = time.perf_counter()
+        impl.backproject(dem, sc.tx, sc.rx, rc, sc.gx, sc.gy, sc.gz, sp.n1, sp.n2, 3e8, sc.fs_eff, sc.lam,
+                         voxels=vox, **kw)
+        return time.perf_counter() - t0
+
+    n0 = max(threads, 1)
+    dt0 = run(n0)
+    n1 = max(n0, int(n0 * seconds / max(dt0, 1e-3)) // n0 * n0)
+    dt1 = run(n1) if n1 > n0 else dt0
+    per_voxel = dt1 / n1
+    full_s = t_pc + t_up + per_voxel * nv_total
+    rate = nv_total * sp.n_pulses / full_s
+    return rate, {"kind": kind, "cores": threads, "sample": (
+        f"{n1} random voxels of the {sp.nx}x{sp.ny}x{sp.nz} grid x {sp.n_pulses} pulses (grid-search Fermat, "
+        f"mean legs, as shipped) in {dt1:.1f} s + full pulse compression {t_pc:.1f} s and upsampling "
+        f"{t_up:.1f} s; rate = full-image voxel-pulses / (compression + upsampling + per-voxel time x "
+        f"{nv_total} voxels)"), "per_voxel_s": per_voxel, "pc_s": t_pc, "upsample_s": t_up}
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU implementation on the box's host cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from bsar import scene as S
+
+    threads = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    sc = make_workload(args.config, 0)
+    sp = sc.spec
+    rates = []
+    details = None
+    for k in range(args.warmup + args.steps):
+        r, details = cpu_reference_rate(sc, args.ref_seconds, threads)
+        if k >= args.warmup:
+            rates.append(r)
+    value = statistics.mean(rates)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": sp.voxel_pulses / value * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded; no dataset)",
+            "config": {"workload": f"{sp.name}: {sp.nx}x{sp.ny}x{sp.nz} voxels, {sp.n_pulses} pulses, "
+                                   f"{sp.n_samples}->{sp.n_samples * sp.upsample} samples, "
+                                   f"{sp.dem_n}^2 fBm DEM", "form": "reference CPU (grid search, mean legs)"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": details["cores"], "kind": details["kind"],
+                             "sample": details["sample"]},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="bsar", choices=["bsar", "reference"])
+    ap.add_argument("--config", type=int, default=2)
+    ap.add_argument("--ref-seconds", type=float, default=15.0, help="CPU work per reference sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip the comparator forms")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        from datetime import timedelta
+
+        dist_mod.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+        dist = dist_mod
+
+    import bsar
+
+    sc = make_workload(args.config, rank)
+    sp = sc.spec
+    stream = torch.cuda.Stream()
+    ctx = bsar.Context(local)
+    ctx.set_stream(stream.cuda_stream)
+    sid = bsar.upload_scene(ctx, sc)
+    W = bsar.scene.search_nodes_for(sc.x_vec, sc.y_vec)
+    nv = sp.n_voxels
+    vp = nv * sp.n_pulses
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if not dist:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---------------- headline: mixed form, inputs resident in HBM -----------------
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        total_ms, bp_ms, img_mixed, launches = time_device(ctx, torch, stream, sid, sc, "mixed", "newton",
+                                                           "per_pulse", args.steps, args.warmup)
+    torch.cuda.synchronize()
+    barrier()
+    total_ms = max_over_ranks(total_ms)
+    ms_per_step = total_ms / args.steps
+    value = world * vp / (ms_per_step / 1e3)
+    bp_avg_ms = max_over_ranks(statistics.mean(bp_ms))
+
+    # ---------------- e2e through the C ABI with host buffers ----------------------
+    raw_pinned = torch.empty(sc.raw.shape, dtype=torch.complex128, pin_memory=True)
+    raw_pinned.numpy()[...] = sc.raw
+    dem = bsar.DemArrays(sc.x_vec, sc.y_vec, sc.z)
+    f0, f1 = -sp.bandwidth / 2, sp.bandwidth / 2
+    img_host = np.empty((sp.nx, sp.ny, sp.nz), dtype=np.complex128)
+
+    def e2e_step():
+        s = ctx.scene_upload(dem, sc.tx, sc.rx, raw_pinned.numpy(), upsample=sp.upsample, n1=sp.n1, n2=sp.n2,
+                             c=3e8, fc=sp.fc, fs=sp.fs, chirp_f0=f0, chirp_f1=f1, chirp_T=sp.pulse_T)
+        out = ctx.backproject(s, sc.gx, sc.gy, sc.gz, solver="newton", legs="per_pulse", precision="mixed")
+        ctx.scene_release(s)
+        return out
+
+    e2e_steps = max(2, min(args.steps, 3))
+    e2e_step()
+    torch.cuda.synchronize()
+    barrier()
+    t = time.perf_counter()
+    for _ in range(e2e_steps):
+        img_host = e2e_step()
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks((time.perf_counter() - t) / e2e_steps)
+    barrier()
+    h2d = (sc.raw.nbytes + sc.tx.nbytes + sc.rx.nbytes + sc.x_vec.nbytes + sc.y_vec.nbytes + sc.z.nbytes
+           + 8 * (len(sc.gx) + len(sc.gy) + len(sc.gz)))
+    d2h = img_host.nbytes
+
+    # ---------------- comparator forms + accuracy ----------------------------------
+    forms = {}
+    acc = {}
+    if not args.no_forms:
+        fs = max(1, min(2, args.steps))
+        t64, bp64, img64, _ = time_device(ctx, torch, stream, sid, sc, "fp64", "newton", "per_pulse", fs, 1)
+        forms["fp64_newton"] = {"value": world * vp / (max_over_ranks(t64 / fs) / 1e3),
+                                "ms_per_step": max_over_ranks(t64 / fs)}
+        t16, _, img16, _ = time_device(ctx, torch, stream, sid, sc, "mixed_fp16", "newton", "per_pulse", fs, 1)
+        forms["mixed_fp16"] = {"value": world * vp / (max_over_ranks(t16 / fs) / 1e3),
+                               "ms_per_step": max_over_ranks(t16 / fs)}
+        # the reference's own algorithm (grid search + mean legs, FP64) on every 20th z-slice
+        gz_sub = sc.gz[::20]
+        tg, _, _, _ = time_device(ctx, torch, stream, sid, sc, "fp64", "grid", "mean", 1, 1, gz=gz_sub)
+        nv_sub = sp.nx * sp.ny * len(gz_sub)
+        forms["fp64_grid_mean_reference_algorithm"] = {
+            "value": world * nv_sub * sp.n_pulses / (max_over_ranks(tg) / 1e3), "ms_per_step": max_over_ranks(tg),
+            "voxels": f"{sp.nx}x{sp.ny}x{len(gz_sub)} (every 20th z-slice)"}
+        forms["mixed_vs_fp64_speedup"] = value / forms["fp64_newton"]["value"]
+        a = img_mixed.cpu().numpy().view(np.complex128).reshape(sp.nx, sp.ny, sp.nz)
+        b = img64.cpu().numpy().view(np.complex128).reshape(sp.nx, sp.ny, sp.nz)
+        c16 = img16.cpu().numpy().view(np.complex128).reshape(sp.nx, sp.ny, sp.nz)
+        m = np.abs(b) >= 1e-3 * np.abs(b).max()
+
+        def stats(x):
+            return {"rel_l2": float(np.linalg.norm(x - b) / np.linalg.norm(b)),
+                    "max_phase_err_rad": float(np.abs(np.angle(x[m] * np.conj(b[m]))).max()),
+                    "argmax_match": bool(np.argmax(np.abs(x)) == np.argmax(np.abs(b)))}
+
+        acc = {"mixed_vs_fp64": stats(a), "mixed_fp16_vs_fp64": stats(c16),
+               "e2e_image_equals_device_image": bool(np.array_equal(img_host, a))}
+
+    # ---------------- roofline of the dominant kernel (k_bp_mixed) ------------------
+    peaks, peak_src = _peaks()
+    clocks = clk.summary()
+    sm_mhz = peaks.get("sm_max_mhz", 1965.0)
+    fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12          # TFLOP/s, FMA = 2 flops
+    flops = fp32_flops_per_voxel_pulse(W) * vp                  # per launch
+    achieved = flops / (bp_avg_ms / 1e3) / 1e12
+    sfu_rate = sfu_ops_per_voxel_pulse(W) * vp / (bp_avg_ms / 1e3)
+    sfu_peak = 148 * 16 * sm_mhz * 1e6
+    roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                "frac": achieved / fp32_peak, "traffic": None,
+                "kernel": "k_bp_mixed", "kernel_ms": bp_avg_ms,
+                "peak_source": f"nominal 148 SM x 128 FP32 lanes x 2 flop x {sm_mhz:.0f} MHz (no FP32-pipe "
+                               f"figure in MEASURED_PEAKS.json)",
+                "sfu": {"achieved_gops": sfu_rate / 1e9, "peak_gops": sfu_peak / 1e9, "frac": sfu_rate / sfu_peak},
+                "gather": {"bytes_per_voxel_pulse": 16, "achieved_gbs": 16 * vp / (bp_avg_ms / 1e3) / 1e9,
+                           "hbm_peak_gbs": peaks.get("hbm_gbs"), "peak_source": peak_src},
+                "fp32_flops_per_voxel_pulse": fp32_flops_per_voxel_pulse(W), "node_scan_half_width": W}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        rate, det = cpu_reference_rate(sc, args.ref_seconds, threads)
+        cpu = {"value": rate, "unit": UNIT, "cores": det["cores"], "kind": det["kind"], "sample": det["sample"]}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64 (mixed)", "data": "synthetic (seeded; no dataset)",
+            "config": {"workload": f"{sp.name}: {sp.nx}x{sp.ny}x{sp.nz} voxels at {sp.dxy} m, {sp.n_pulses} pulses, "
+                                   f"{sp.n_samples}->{sp.n_samples * sp.upsample} fast-time samples, "
+                                   f"{sp.dem_n}^2 fBm DEM ({sp.dem_d} m, sigma {sp.dem_sigma} m), eps_r {sp.eps_r}, "
+                                   f"{sp.n_scatterers} scatterers, {sp.snr_db} dB",
+                       "form": "mixed (Newton Fermat FP32 + FP64 final step, complex64 samples, Kahan FP32 sums)",
+                       "per_gpu": "one z-slab of the full grid size per rank",
+                       "l2": "inputs larger than L2 (upsampled complex64 pulses "
+                             f"{sp.n_pulses * sp.n_samples * sp.upsample * 8 / 2**20:.0f} MiB)",
+                       "parallelism": f"voxel slabs x{world}, no collective"},
+            "e2e": {"value": world * vp / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_s * 1e3},
+            "gpu_launches": int(launches),
+            "roofline": roofline,
+            "forms": forms,
+            "accuracy": acc,
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.scene_release(sid)
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -279,6 +279,7 @@ struct Scene {
     std::unique_ptr<DevBuf> tx, rx, samples;
     std::vector<double> reference;     // matched-filter reference (Ns complex), RAW scenes
     RcBuf rc[3];                       // per bsar_precision
+    std::unique_ptr<DevBuf> spec[3];   // matched-filter spectrum per precision (bit-reversed)
     // mixed-form anchors (per grid centre and node-scan width)
     std::unique_ptr<DevBuf> anchors;
     double anchor_key[4] = {NAN, NAN, NAN, NAN};
@@ -358,20 +359,25 @@ static void compress_scene(bsar_ctx* ctx, Scene* s, int precision)
         fail(BSAR_ERR_UNSUPPORTED, "pulse length %lld exceeds the single-CTA FFT (%lld for this precision)",
              (long long)s->ns, (long long)max_fft_len(a.real_bytes));
     a.tw = twiddles(ctx, a.P, a.real_bytes);
-    auto spec = dev_alloc(ctx, (size_t)a.P * (a.real_bytes == 8 ? sizeof(double2) : sizeof(float2)));
-    std::vector<double> ref = s->reference;
-    if (s->kind == BSAR_SAMPLES_COMPRESSED) {
-        // delta reference: its spectrum is all ones, the filter is the identity
-        ref.assign(2 * (size_t)s->ns, 0.0);
-        ref[0] = 1.0;
+    std::unique_ptr<DevBuf>& spec = s->spec[precision];
+    if (!spec) {
+        // the reference's spectrum once per scene and precision (the reference recomputes
+        // it for every pulse, src/fft_utils.cpp:81-82)
+        spec = dev_alloc(ctx, (size_t)a.P * (a.real_bytes == 8 ? sizeof(double2) : sizeof(float2)));
+        std::vector<double> ref = s->reference;
+        if (s->kind == BSAR_SAMPLES_COMPRESSED) {
+            // delta reference: its spectrum is all ones, the filter is the identity
+            ref.assign(2 * (size_t)s->ns, 0.0);
+            ref[0] = 1.0;
+        }
+        auto dref = dev_upload(ctx, ref.data(), sizeof(double) * ref.size());
+        launched(ctx, launch_ref_spectrum(dref->as<double2>(), (int)s->ns, a.P, a.logP, a.tw, 1, spec->p,
+                                          a.real_bytes, ctx->stream),
+                 "reference spectrum");
+        sync(ctx);
     }
-    auto dref = dev_upload(ctx, ref.data(), sizeof(double) * ref.size());
-    launched(ctx, launch_ref_spectrum(dref->as<double2>(), (int)s->ns, a.P, a.logP, a.tw, 1, spec->p, a.real_bytes,
-                                      ctx->stream),
-             "reference spectrum");
     a.spec = spec->p;
     launched(ctx, launch_pulse_compress(a, ctx->stream), "pulse compression");
-    sync(ctx);
 }
 
 // ------------------------------------------------------------------------------------
