@@ -196,11 +196,12 @@ class Context:
         self._ok(self.L.bsar_dem_elevation(self.h, C.byref(dem.c), _p(xy), len(xy), _p(out)))
         return out
 
-    def refraction_points(self, dem: DemArrays, p1, p2, n1, n2, solver="grid", search_radius_m=0.0):
+    def refraction_points(self, dem: DemArrays, p1, p2, n1, n2, solver="grid", search_radius_m=0.0,
+                          precision="fp64"):
         p1 = _f64(p1, (-1, 3))
         p2 = _f64(p2, (-1, 3))
         out = np.empty((len(p1), 3))
-        fo = FermatOpts(SOLVER[solver], 0, search_radius_m)
+        fo = FermatOpts(SOLVER[solver], PRECISION[precision], search_radius_m)
         self._ok(self.L.bsar_refraction_points(self.h, C.byref(dem.c), _p(p1), _p(p2), len(p1), n1, n2,
                                                C.byref(fo), _p(out)))
         return out

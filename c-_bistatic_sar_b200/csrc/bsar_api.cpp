@@ -6,7 +6,9 @@
 // results back.  There is no host-side compute path: every result comes from a kernel.
 #include "bsar.h"
 
+#include <cuda.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cmath>
@@ -84,6 +86,8 @@ struct bsar_ctx {
     // cached grid axes for the asynchronous entry point
     std::vector<double> grid_host;
     std::unique_ptr<DevBuf> grid_dev;
+    // device status word raised by bounded device-side waits
+    std::unique_ptr<DevBuf> status;
 };
 
 struct DevBuf {
@@ -135,13 +139,61 @@ static void launched(bsar_ctx* ctx, cudaError_t e, const char* what)
 
 static void sync(bsar_ctx* ctx) { cuda_check(cudaStreamSynchronize(ctx->stream), "stream synchronize"); }
 
+// A bounded device-side wait that ran out raises the context's status word.
+static void check_device_status(bsar_ctx* ctx)
+{
+    if (!ctx->status) return;
+    int h = 0;
+    cuda_check(cudaMemcpy(&h, ctx->status->p, sizeof(int), cudaMemcpyDeviceToHost), "status read");
+    if (h) {
+        cuda_check(cudaMemset(ctx->status->p, 0, sizeof(int)), "status reset");
+        fail(BSAR_ERR_TIMEOUT, "a device-side DEM tile copy did not complete within its wait limit");
+    }
+}
+
+
 // ------------------------------------------------------------------------------------
 // DEM staging
 // ------------------------------------------------------------------------------------
 struct DemDev {
     std::unique_ptr<DevBuf> xv, yv, z, z32;
     DemView view{};
+    int pitch = 0;                                  // row pitch of z32 (floats, multiple of 4)
+    alignas(64) unsigned char tmap[sizeof(CUtensorMap)] = {};
+    bool has_tmap = false;
 };
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link to libcuda).
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        cudaGetLastError();
+    }
+    return fn;
+}
+
+// Tensor map of the FP32 DEM for the mixed kernel's TMA tile loads.
+static bool make_dem_tmap(DemDev& r)
+{
+    auto enc = tensor_map_encoder();
+    if (!enc || !r.z32) return false;
+    cuuint64_t dims[2] = {(cuuint64_t)r.view.nx, (cuuint64_t)r.view.ny};
+    cuuint64_t strides[1] = {(cuuint64_t)r.pitch * sizeof(float)};
+    cuuint32_t box[2] = {(cuuint32_t)kMixedTileI, (cuuint32_t)kMixedTileJ};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult e = enc(reinterpret_cast<CUtensorMap*>(r.tmap), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, r.z32->p, dims,
+                     strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return e == CUDA_SUCCESS;
+}
 
 static void check_dem(const bsar_dem* d)
 {
@@ -200,11 +252,15 @@ static DemDev stage_dem(bsar_ctx* ctx, const bsar_dem* d, bool want_z32)
     v.stepx = d->nx > 1 ? (d->x_vec[d->nx - 1] - d->x_vec[0]) / (double)(d->nx - 1) : 1.0;
     v.stepy = d->ny > 1 ? (d->y_vec[d->ny - 1] - d->y_vec[0]) / (double)(d->ny - 1) : 1.0;
     if (want_z32) {
-        std::vector<float> zf((size_t)d->nx * d->ny);
-        for (size_t k = 0; k < zf.size(); k++) zf[k] = (float)d->z[k];
+        // rows padded to a multiple of 4 floats: 16-byte tensor-map strides
+        r.pitch = (int)((d->nx + 3) & ~int64_t(3));
+        std::vector<float> zf((size_t)r.pitch * d->ny, 0.0f);
+        for (int64_t j = 0; j < d->ny; j++)
+            for (int64_t i = 0; i < d->nx; i++) zf[j * r.pitch + i] = (float)d->z[j * d->nx + i];
         r.z32 = dev_upload(ctx, zf.data(), sizeof(float) * zf.size());
         sync(ctx);   // zf goes out of scope
         v.z32 = r.z32->as<float>();
+        if (d->nx >= 2 && d->ny >= 2) r.has_tmap = make_dem_tmap(r);
     }
     return r;
 }
@@ -283,6 +339,7 @@ struct Scene {
     // mixed-form anchors (per grid centre and node-scan width)
     std::unique_ptr<DevBuf> anchors;
     double anchor_key[4] = {NAN, NAN, NAN, NAN};
+    float off_x = 0.f, off_y = 0.f;    // mean crossing offset from the grid centre
 };
 
 static Scene* get_scene(bsar_ctx* ctx, bsar_scene_id id)
@@ -474,7 +531,13 @@ bsar_status bsar_set_stream(bsar_ctx* ctx, void* stream)
     });
 }
 
-bsar_status bsar_synchronize(bsar_ctx* ctx) { return guarded(ctx, [&] { sync(ctx); }); }
+bsar_status bsar_synchronize(bsar_ctx* ctx)
+{
+    return guarded(ctx, [&] {
+        sync(ctx);
+        check_device_status(ctx);
+    });
+}
 
 uint64_t bsar_launch_count(const bsar_ctx* ctx) { return ctx ? ctx->launches : 0; }
 uint64_t bsar_bytes_in_use(const bsar_ctx* ctx) { return ctx ? ctx->used : 0; }
@@ -502,18 +565,27 @@ bsar_status bsar_refraction_points(bsar_ctx* ctx, const bsar_dem* dem, const dou
         if (n < 0 || (n > 0 && (!p1 || !p2 || !out))) fail(BSAR_ERR_INVALID_ARG, "bad point buffers");
         int solver = fermat_solver(fopts);
         if (solver != BSAR_SOLVER_GRID && solver != BSAR_SOLVER_NEWTON) fail(BSAR_ERR_INVALID_ARG, "unknown solver");
-        if (fopts && fopts->precision != BSAR_FP64)
-            fail(BSAR_ERR_UNSUPPORTED, "crossing points are returned by the FP64 solvers");
+        const int prec = fopts ? fopts->precision : BSAR_FP64;
+        if (prec != BSAR_FP64 && prec != BSAR_MIXED) fail(BSAR_ERR_INVALID_ARG, "unknown precision");
+        if (prec == BSAR_MIXED && solver != BSAR_SOLVER_NEWTON)
+            fail(BSAR_ERR_UNSUPPORTED, "the mixed solver is the Newton solver");
         if (n == 0) return;
-        DemDev d = stage_dem(ctx, dem, false);
+        DemDev d = stage_dem(ctx, dem, prec == BSAR_MIXED);
         if (solver == BSAR_SOLVER_NEWTON) check_newton_dem(d.view);
+        if (prec == BSAR_MIXED && (d.view.empty || d.view.nx < 2 || d.view.ny < 2))
+            fail(BSAR_ERR_UNSUPPORTED, "the mixed solver needs a DEM of at least 2 x 2 nodes");
         int W = search_nodes(d.view, fopts ? fopts->search_radius_m : 0.0);
         auto a = dev_upload(ctx, p1, sizeof(double) * 3 * n);
         auto b = dev_upload(ctx, p2, sizeof(double) * 3 * n);
         auto o = dev_alloc(ctx, sizeof(double) * 3 * n);
-        launched(ctx, launch_refraction_points(d.view, a->as<double>(), b->as<double>(), n, n1, n2, solver, W,
-                                               o->as<double>(), ctx->stream),
-                 "refraction points");
+        if (prec == BSAR_MIXED)
+            launched(ctx, launch_refraction_mixed(d.view, d.pitch, a->as<double>(), b->as<double>(), n, n1, n2, W,
+                                                  o->as<double>(), ctx->stream),
+                     "refraction points (mixed)");
+        else
+            launched(ctx, launch_refraction_points(d.view, a->as<double>(), b->as<double>(), n, n1, n2, solver, W,
+                                                   o->as<double>(), ctx->stream),
+                     "refraction points");
         cuda_check(cudaMemcpyAsync(out, o->p, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, ctx->stream), "download");
         sync(ctx);
     });
@@ -800,11 +872,24 @@ static void backproject(bsar_ctx* ctx, bsar_scene_id id, const bsar_grid* g, con
     int64_t np = s->np;
     if (!s->anchors || std::memcmp(key, s->anchor_key, sizeof key) != 0) {
         s->anchors = dev_alloc(ctx, (sizeof(double) + sizeof(float) + sizeof(int) + sizeof(float)) * np);
+        auto offs = dev_alloc(ctx, sizeof(double) * 4 * np);
         char* base = s->anchors->as<char>();
         launched(ctx, launch_ref_ranges(s->dem.view, a.tx, a.rx, (int)np, centre, s->n1, s->n2, a.W, a.lambda,
                                         a.fs_eff / s->c, (double*)base, (float*)(base + 8 * np),
-                                        (int*)(base + 12 * np), (float*)(base + 16 * np), ctx->stream),
+                                        (int*)(base + 12 * np), (float*)(base + 16 * np), offs->as<double>(),
+                                        ctx->stream),
                  "reference ranges");
+        std::vector<double> h(4 * np);
+        cuda_check(cudaMemcpyAsync(h.data(), offs->p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, ctx->stream),
+                   "d2h");
+        sync(ctx);
+        double ox = 0, oy = 0;
+        for (int64_t i = 0; i < np; i++) {
+            ox += h[4 * i] + h[4 * i + 2];
+            oy += h[4 * i + 1] + h[4 * i + 3];
+        }
+        s->off_x = (float)(ox / (2.0 * np));
+        s->off_y = (float)(oy / (2.0 * np));
         std::memcpy(s->anchor_key, key, sizeof key);
     }
     char* base = s->anchors->as<char>();
@@ -812,7 +897,13 @@ static void backproject(bsar_ctx* ctx, bsar_scene_id id, const bsar_grid* g, con
     a.ref_phase = (const float*)(base + 8 * np);
     a.ref_bin_i = (const int*)(base + 12 * np);
     a.ref_bin_f = (const float*)(base + 16 * np);
-    cudaError_t e = launch_bp_mixed(a, o->legs, o->precision == BSAR_MIXED_FP16 ? 1 : 0, ctx->stream);
+    if (!ctx->status) {
+        ctx->status = dev_alloc(ctx, sizeof(int));
+        cuda_check(cudaMemsetAsync(ctx->status->p, 0, sizeof(int), ctx->stream), "memset");
+    }
+    MixedLaunch ml{s->dem.pitch, s->dem.has_tmap ? (const void*)s->dem.tmap : nullptr, s->off_x, s->off_y,
+                   ctx->status->as<int>()};
+    cudaError_t e = launch_bp_mixed(a, ml, o->legs, o->precision == BSAR_MIXED_FP16 ? 1 : 0, ctx->stream);
     if (e == cudaErrorNotSupported) {
         cudaGetLastError();
         fail(BSAR_ERR_UNSUPPORTED, "mixed back-projection mode not supported");
@@ -831,6 +922,7 @@ bsar_status bsar_backproject(bsar_ctx* ctx, bsar_scene_id id, const bsar_grid* g
         backproject(ctx, id, g, o, img->as<double2>());
         cuda_check(cudaMemcpyAsync(image_out, img->p, sizeof(double2) * nv, cudaMemcpyDeviceToHost, ctx->stream), "d2h");
         sync(ctx);
+        check_device_status(ctx);
     });
 }
 

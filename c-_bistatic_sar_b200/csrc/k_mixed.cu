@@ -1,14 +1,23 @@
 // k_mixed.cu -- the mixed-precision back-projection kernel.
 //
-// One thread per voxel, voxels of a warp consecutive in the reference's flat order
+// One thread per voxel, voxels of a CTA consecutive in the reference's flat order
 // (y fastest), every thread walking the pulses in order.  Lanes of a warp solve the same
 // pulse for neighbouring voxels, so their DEM windows, Tx/Rx loads and sample gathers
 // coincide or sit next to each other.
 //
+// DEM tile: at start every CTA stages a TI x TJ FP32 tile of the DEM around its voxels
+// (shifted by the scene's mean crossing offset) into shared memory with one TMA 2-D
+// tiled load (cp.async.bulk.tensor, no multicast) completing on an mbarrier; node scans
+// whose window lies inside the tile read it from there, others read the FP32 DEM in
+// global memory.
+//
 // Per (voxel, pulse):
 //   Fermat, twice (Tx -> voxel, voxel -> Rx):
-//     FP32  flat-interface start, node scan of +-W DEM nodes, active-set Newton polish
-//           on the 4 facets around the best node (coordinates relative to the DEM origin)
+//     FP32  flat-interface start; node scan of the (2W+1)^2 DEM nodes around it
+//           (compile-time W for the common widths) ranking na|N-A| + nb|N-B|; when the
+//           runner-up is within kTieM metres of the best, the candidates within kTieM are
+//           re-ranked in FP64 with the FP64 solver's arithmetic and scan order, so both
+//           forms pick the same node; active-set Newton polish on the 4 facets around it
 //     FP64  one final Newton step on the winning facet; its leg lengths give the
 //           bistatic optical path L in FP64
 //   delay / phase: dL = L - L_ref(pulse) rounded to FP32; the fast-time bin and carrier
@@ -16,6 +25,7 @@
 //           phase reduced to [-pi, pi) in FP64)
 //   gather: two complex64 (or FP16 complex x pulse scale) samples, linear interpolation
 //           (proc_test_script.cpp:589-636), times exp(j phi), Kahan-compensated FP32 sum.
+#include <cuda.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
@@ -28,18 +38,32 @@ namespace bsar {
 
 namespace {
 
+constexpr int TI = kMixedTileI;    // tile columns (x); 272 B rows, a multiple of 16 B
+constexpr int TJ = kMixedTileJ;    // tile rows (y)
+constexpr float kTieM = 1.0e-4f;   // metres: FP32 node-scan ranking ambiguity threshold
+constexpr float kStartBand = 2.0e-3f;  // node units: FP32 start too close to a cell boundary
+constexpr long kWaitSpins = 1L << 24;
+
 struct Facet32 {
     float x0, y0, dx, dy, z00, b, c, e;
 };
 
 struct MixedCtx {
-    const float* __restrict__ z32;
+    const float* __restrict__ z32;  // pitch-padded FP32 heights, z32[j * pitch + i]
+    int pitch;
     int nx, ny;
-    float stepx, stepy;      // uniform node spacing
-    double ox, oy;           // origin of the FP32 frame (first DEM node)
+    float stepx, stepy;             // uniform node spacing
+    double ox, oy;                  // origin of the FP32 frame (first DEM node)
 };
 
-__device__ __forceinline__ float zf(const MixedCtx& m, int i, int j) { return __ldg(m.z32 + (int64_t)j * m.nx + i); }
+// A DEM tile in shared memory: node (i, j) at s[(j - j0) * TI + (i - i0)].
+struct Tile {
+    const float* s;
+    int i0, j0;
+    bool ok;
+};
+
+__device__ __forceinline__ float zf(const MixedCtx& m, int i, int j) { return __ldg(m.z32 + (int64_t)j * m.pitch + i); }
 
 // FP32 bilinear height (clamped to the DEM) for the flat-interface start.
 __device__ __forceinline__ float height32(const MixedCtx& m, float x, float y)
@@ -118,7 +142,8 @@ __device__ __forceinline__ float facet_eval32(const Facet32& F, const float A[3]
 // FP64 final Newton step on facet (fi, fj) from (u, v); returns the optical path of the
 // result and its two leg lengths (|X-A|, |X-B|).
 __device__ __forceinline__ double final_step64(const DemView& d, int fi, int fj, const double A[3], const double B[3],
-                                               double na, double nb, double u, double v, double& dA, double& dB)
+                                               double na, double nb, double u, double v, double& dA, double& dB,
+                                               double* X)
 {
     Facet64 F;
     facet_load(d, fi, fj, F);
@@ -176,14 +201,176 @@ __device__ __forceinline__ double final_step64(const DemView& d, int fi, int fj,
     double r2x = x - B[0], r2y = y - B[1], r2z = h - B[2];
     dA = sqrt(r1x * r1x + r1y * r1y + r1z * r1z);
     dB = sqrt(r2x * r2x + r2y * r2y + r2z * r2z);
+    if (X) {
+        X[0] = x;
+        X[1] = y;
+        X[2] = h;
+    }
     return na * dA + nb * dB;
 }
 
+// Node optical path in FP64 with the FP64 solver's exact arithmetic (no contraction):
+// na*sqrt(|N-A|^2) + nb*sqrt(|N-B|^2), sums and products in the same order.
+__device__ __forceinline__ double node_l64(const DemView& d, int i, int j, const double A[3], const double B[3],
+                                           double na, double nb)
+{
+    double xi = __ldg(d.xv + i), yj = __ldg(d.yv + j), zij = __ldg(d.z + (int64_t)j * d.nx + i);
+    double r1x = __dsub_rn(xi, A[0]), r1y = __dsub_rn(yj, A[1]), r1z = __dsub_rn(zij, A[2]);
+    double r2x = __dsub_rn(xi, B[0]), r2y = __dsub_rn(yj, B[1]), r2z = __dsub_rn(zij, B[2]);
+    double q1 = __dadd_rn(__dadd_rn(__dmul_rn(r1x, r1x), __dmul_rn(r1y, r1y)), __dmul_rn(r1z, r1z));
+    double q2 = __dadd_rn(__dadd_rn(__dmul_rn(r2x, r2x), __dmul_rn(r2y, r2y)), __dmul_rn(r2z, r2z));
+    return __dadd_rn(__dmul_rn(na, __dsqrt_rn(q1)), __dmul_rn(nb, __dsqrt_rn(q2)));
+}
+
+// Scaled FP32 node path |N-A| + rb |N-B| (rb = nb / na; ranking is scale-free).
+__device__ __forceinline__ float node_l32(float z, float sxa, float sya, float sxb, float syb, float Az, float Bz,
+                                          float rb)
+{
+    float dza = z - Az, dzb = z - Bz;
+    float qa = fmaf(dza, dza, sxa + sya);
+    float qb = fmaf(dzb, dzb, sxb + syb);
+    return fmaf(rb, qb * rsqrtf(qb), qa * rsqrtf(qa));
+}
+
+// Branch-free ranking update: best value / index and runner-up value.
+__device__ __forceinline__ void rank(float L, int i, int j, float& v1, float& v2, int& bi, int& bj)
+{
+    v2 = fminf(v2, fmaxf(v1, L));
+    bool p = L < v1;
+    v1 = p ? L : v1;
+    bi = p ? i : bi;
+    bj = p ? j : bj;
+}
+
+// Node scan over [ia, ib] x [ja, jb] (clamped window), generic width; z from the tile
+// when `in_tile`, else from global memory.
+struct Rank {
+    float v1, v2;
+    int bi, bj;
+};
+
+__device__ __noinline__ Rank scan_generic(const MixedCtx m, const float* ts, int ti0, int tj0, bool in_tile, int ia,
+                                          int ib, int ja, int jb, float ax, float ay, float az, float bx, float by,
+                                          float bz, float rb, Rank r)
+{
+    for (int i = ia; i <= ib; i++) {
+        float xi = (float)i * m.stepx;
+        float dxa = xi - ax, dxb = xi - bx;
+        float sxa = dxa * dxa, sxb = dxb * dxb;
+        for (int j = ja; j <= jb; j++) {
+            float yj = (float)j * m.stepy;
+            float dya = yj - ay, dyb = yj - by;
+            float z = in_tile ? ts[(j - tj0) * TI + (i - ti0)] : zf(m, i, j);
+            rank(node_l32(z, sxa, dya * dya, sxb, dyb * dyb, az, bz, rb), i, j, r.v1, r.v2, r.bi, r.bj);
+        }
+    }
+    return r;
+}
+
+// Full (2W+1)^2 window inside the DEM and inside the tile: per-column terms in registers,
+// fully unrolled columns, tile reads at compile-time offsets.
+template <int W>
+__device__ __forceinline__ void scan_tile(const MixedCtx& m, const Tile& T, int is, int js, const float A[3],
+                                          const float B[3], float rb, float& v1, float& v2, int& bi, int& bj)
+{
+    constexpr int NJ = 2 * W + 1;
+    float sya[NJ], syb[NJ];
+#pragma unroll
+    for (int c = 0; c < NJ; c++) {
+        float yj = (float)(js - W + c) * m.stepy;
+        float dya = yj - A[1], dyb = yj - B[1];
+        sya[c] = dya * dya;
+        syb[c] = dyb * dyb;
+    }
+    const float* col0 = T.s + (js - W - T.j0) * TI - T.i0;
+#pragma unroll 1
+    for (int i = is - W; i <= is + W; i++) {
+        float xi = (float)i * m.stepx;
+        float dxa = xi - A[0], dxb = xi - B[0];
+        float sxa = dxa * dxa, sxb = dxb * dxb;
+        const float* zc = col0 + i;
+#pragma unroll
+        for (int c = 0; c < NJ; c++)
+            rank(node_l32(zc[c * TI], sxa, sya[c], sxb, syb[c], A[2], B[2], rb), i, js - W + c, v1, v2, bi, bj);
+    }
+}
+
+template <int W>
+__device__ __forceinline__ void node_scan(const MixedCtx& m, const Tile& T, int is, int js, int Wr, const float A[3],
+                                          const float B[3], float rb, float& v1, float& v2, int& bi, int& bj)
+{
+    const int ia = max(is - Wr, 0), ib = min(is + Wr, m.nx - 1);
+    const int ja = max(js - Wr, 0), jb = min(js + Wr, m.ny - 1);
+    const bool in_tile = T.ok && ia >= T.i0 && ib < T.i0 + TI && ja >= T.j0 && jb < T.j0 + TJ;
+    if constexpr (W > 0) {
+        if (in_tile && Wr == W && ia == is - W && ib == is + W && ja == js - W && jb == js + W) {
+            scan_tile<W>(m, T, is, js, A, B, rb, v1, v2, bi, bj);
+            return;
+        }
+    }
+    Rank r = scan_generic(m, T.s, T.i0, T.j0, in_tile, ia, ib, ja, jb, A[0], A[1], A[2], B[0], B[1], B[2], rb,
+                          Rank{v1, v2, bi, bj});
+    v1 = r.v1;
+    v2 = r.v2;
+    bi = r.bi;
+    bj = r.bj;
+}
+
+// FP64 re-ranking of the nodes within the FP32 ambiguity band, in the FP64 solver's
+// order (i-major, j-minor, strict <).
+__device__ __noinline__ int2 rerank64(const DemView d, const MixedCtx m, const float* ts, int ti0, int tj0, bool tok,
+                                      int is, int js, int Wr, float ax, float ay, float az, float bx, float by,
+                                      float bz, float rb, float limit, double Ax, double Ay, double Az, double Bx,
+                                      double By, double Bz, double na, double nb, int2 best_ij)
+{
+    const int ia = max(is - Wr, 0), ib = min(is + Wr, m.nx - 1);
+    const int ja = max(js - Wr, 0), jb = min(js + Wr, m.ny - 1);
+    const bool in_tile = tok && ia >= ti0 && ib < ti0 + TI && ja >= tj0 && jb < tj0 + TJ;
+    const double A[3] = {Ax, Ay, Az}, B[3] = {Bx, By, Bz};
+    double best = INFINITY;
+    for (int i = ia; i <= ib; i++) {
+        float xi = (float)i * m.stepx;
+        float dxa = xi - ax, dxb = xi - bx;
+        float sxa = dxa * dxa, sxb = dxb * dxb;
+        for (int j = ja; j <= jb; j++) {
+            float yj = (float)j * m.stepy;
+            float dya = yj - ay, dyb = yj - by;
+            float z = in_tile ? ts[(j - tj0) * TI + (i - ti0)] : zf(m, i, j);
+            if (node_l32(z, sxa, dya * dya, sxb, dyb * dyb, az, bz, rb) <= limit) {
+                double L = node_l64(d, i, j, A, B, na, nb);
+                if (L < best) {
+                    best = L;
+                    best_ij = make_int2(i, j);
+                }
+            }
+        }
+    }
+    return best_ij;
+}
+
+// FP64 flat-interface start and its nearest node, exactly as the FP64 solver makes them
+// (used when the FP32 start lies within rounding distance of a node-cell boundary).
+__device__ __noinline__ int2 start_node64(const DemView d, double Ax, double Ay, double Az, double Bx, double By,
+                                          double Bz, double na, double nb)
+{
+    const double A[3] = {Ax, Ay, Az}, B[3] = {Bx, By, Bz};
+    const bool lower_b = nb >= na;
+    const double* Lp = lower_b ? B : A;
+    const double* Up = lower_b ? A : B;
+    double nl = lower_b ? nb : na, nu = lower_b ? na : nb;
+    double h0 = dem_elevation(d, Lp[0], Lp[1]);
+    double sx, sy;
+    flat_start(Up, Lp, nu, nl, h0, kFlatIters, sx, sy);
+    return make_int2(nearest_node(d.x0, d.stepx, d.nx, sx), nearest_node(d.y0, d.stepy, d.ny, sy));
+}
+
 // Mixed-precision crossing solve A (index na) -> B (index nb).  A32/B32: the endpoints in
-// the FP32 frame.  Returns the FP64 optical path; dA, dB: FP64 leg lengths.
-__device__ __forceinline__ double solve_mixed(const DemView& d, const MixedCtx& m, const double A[3],
-                                              const double B[3], const float A32[3], const float B32[3],
-                                              float na, float nb, int W, double& dA, double& dB)
+// the FP32 frame.  Returns the FP64 optical path; dA, dB: FP64 leg lengths; X (optional):
+// the crossing point.
+template <int WT>
+__device__ __forceinline__ double solve_mixed(const DemView& d, const MixedCtx& m, const Tile& T, const double A[3],
+                                              const double B[3], const float A32[3], const float B32[3], float na,
+                                              float nb, int W, double& dA, double& dB, double* X = nullptr)
 {
     // 1. flat-interface start (FP32)
     const bool lower_b = nb >= na;
@@ -208,32 +395,28 @@ __device__ __forceinline__ double solve_mixed(const DemView& d, const MixedCtx& 
         sx = Up[0] + hx * (s / D);
         sy = Up[1] + hy * (s / D);
     }
-    // 2. node scan (FP32), strict < in i-major, j-minor order
-    int is = min(max(__float2int_rn(sx / m.stepx), 0), m.nx - 1);
-    int js = min(max(__float2int_rn(sy / m.stepy), 0), m.ny - 1);
-    int ia = max(is - W, 0), ib = min(is + W, m.nx - 1);
-    int ja = max(js - W, 0), jb = min(js + W, m.ny - 1);
-    float bestL = INFINITY;
+    // 2. node scan (FP32, scaled by 1/na), FP64 re-rank of near ties.  The window centre is
+    //    the node nearest the start; a start within rounding distance of a cell boundary
+    //    is redone in FP64 so both forms scan the same window.
+    const float fx = sx / m.stepx, fy = sy / m.stepy;
+    int is = min(max(__float2int_rn(fx), 0), m.nx - 1);
+    int js = min(max(__float2int_rn(fy), 0), m.ny - 1);
+    if (fabsf(fabsf(fx - rintf(fx)) - 0.5f) < kStartBand || fabsf(fabsf(fy - rintf(fy)) - 0.5f) < kStartBand) {
+        const int2 s64 = start_node64(d, A[0], A[1], A[2], B[0], B[1], B[2], (double)na, (double)nb);
+        is = s64.x;
+        js = s64.y;
+    }
+    const float rb = nb / na;
+    float v1 = INFINITY, v2 = INFINITY;
     int bi = is, bj = js;
-    for (int i = ia; i <= ib; i++) {
-        float xi = (float)i * m.stepx;
-        float dxa = xi - A32[0], dxb = xi - B32[0];
-        float sxa = dxa * dxa, sxb = dxb * dxb;
-        const float* zrow = m.z32 + i;
-        for (int j = ja; j <= jb; j++) {
-            float yj = (float)j * m.stepy;
-            float zij = __ldg(zrow + (int64_t)j * m.nx);
-            float dya = yj - A32[1], dyb = yj - B32[1];
-            float dza = zij - A32[2], dzb = zij - B32[2];
-            float qa = fmaf(dza, dza, fmaf(dya, dya, sxa));
-            float qb = fmaf(dzb, dzb, fmaf(dyb, dyb, sxb));
-            float L = na * (qa * rsqrtf(qa)) + nb * (qb * rsqrtf(qb));
-            if (L < bestL) {
-                bestL = L;
-                bi = i;
-                bj = j;
-            }
-        }
+    node_scan<WT>(m, T, is, js, W, A32, B32, rb, v1, v2, bi, bj);
+    const float tie = kTieM / na;
+    if (!(v2 - v1 >= tie)) {
+        const int2 b = rerank64(d, m, T.s, T.i0, T.j0, T.ok, is, js, W, A32[0], A32[1], A32[2], B32[0], B32[1], B32[2],
+                                rb, v1 + tie, A[0], A[1], A[2], B[0], B[1], B[2], (double)na, (double)nb,
+                                make_int2(bi, bj));
+        bi = b.x;
+        bj = b.y;
     }
     // 3. polish the facets around the best node (FP32)
     int bfi = min(bi, m.nx - 2), bfj = min(bj, m.ny - 2);     // fallback facet
@@ -266,14 +449,72 @@ __device__ __forceinline__ double solve_mixed(const DemView& d, const MixedCtx& 
         }
     }
     // 4. FP64 final step
-    return final_step64(d, bfi, bfj, A, B, (double)na, (double)nb, (double)bu, (double)bv, dA, dB);
+    return final_step64(d, bfi, bfj, A, B, (double)na, (double)nb, (double)bu, (double)bv, dA, dB, X);
 }
+
+// ------------------------------- TMA tile staging -----------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint32_t mbar_try_wait(uint32_t bar)
+{
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(bar)
+        : "memory");
+    return done;
+}
+
+// One elected thread loads the tile with a TMA 2-D tiled copy completing on `mbar`;
+// every thread then waits with a bounded spin.  Returns false (and raises *status) if
+// the copy did not complete in time.
+__device__ bool stage_tile(const CUtensorMap* tmap, float* tile, uint64_t* mbar, int i0, int j0, int* status)
+{
+    const uint32_t bar = smem_u32(mbar);
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const uint32_t bytes = TI * TJ * sizeof(float);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+        asm volatile(
+            "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+                "r"(smem_u32(tile)), "l"(reinterpret_cast<uint64_t>(tmap)), "r"(i0), "r"(j0), "r"(bar)
+            : "memory");
+    }
+    uint32_t done = 0;
+    for (long s = 0; s < kWaitSpins && !done; s++) done = mbar_try_wait(bar);
+    if (!done && status) atomicExch(status, 1);
+    return done != 0;
+}
+
+// A copy that missed its deadline may still be in flight: wait for it (bounded) before
+// the CTA's shared memory is released.
+__device__ void drain_tile(uint64_t* mbar)
+{
+    const uint32_t bar = smem_u32(mbar);
+    uint32_t done = 0;
+    for (long s = 0; s < kWaitSpins && !done; s++) done = mbar_try_wait(bar);
+}
+
+struct MixedExtra {
+    float off_x, off_y;   // mean crossing offset from the voxel (m), tile centring
+    int* status;          // device status word: 1 = a tile copy timed out
+    int use_tile;
+};
 
 }  // namespace
 
-template <int FP16>
-__global__ void __launch_bounds__(128) k_bp_mixed(BpArgs a, MixedCtx m)
+template <int FP16, int WT>
+__global__ void __launch_bounds__(128, 4) k_bp_mixed(BpArgs a, MixedCtx m, MixedExtra ex,
+                                                  const __grid_constant__ CUtensorMap tmap)
 {
+    __shared__ alignas(128) float tile_s[TI * TJ];
+    __shared__ alignas(8) uint64_t mbar;
     const int* __restrict__ ref_bin_i = a.ref_bin_i;
     const float* __restrict__ ref_bin_f = a.ref_bin_f;
     const int np = a.np;
@@ -281,8 +522,23 @@ __global__ void __launch_bounds__(128) k_bp_mixed(BpArgs a, MixedCtx m)
     const float k_phase = (float)(2.0 * 3.14159265358979323846 / a.lambda);
     const float n1f = (float)a.n1, n2f = (float)a.n2;
     const int64_t nr = a.nr;
-    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < a.v_count;
-         k += (int64_t)gridDim.x * blockDim.x) {
+
+    // tile centred on this CTA's voxels plus the scene's mean crossing offset
+    Tile T{tile_s, 0, 0, false};
+    if (ex.use_tile) {
+        const int64_t v0 = a.v_begin + (int64_t)blockIdx.x * blockDim.x;
+        const int64_t vl = min(v0 + (int64_t)blockDim.x, a.v_begin + a.v_count) - 1;
+        const int64_t vm = (v0 + vl) / 2;
+        const double cx = __ldg(a.gx + (int)((vm / a.ny) % a.nx)) + ex.off_x;
+        const double cy = __ldg(a.gy + (int)(vm % a.ny)) + ex.off_y;
+        const int ci = (int)floor((cx - m.ox) / m.stepx), cj = (int)floor((cy - m.oy) / m.stepy);
+        T.i0 = ((ci - TI / 2) >> 2) << 2;      // TMA: x offset a multiple of 4 floats (16 B)
+        T.j0 = cj - TJ / 2;
+        T.ok = stage_tile(&tmap, tile_s, &mbar, T.i0, T.j0, ex.status);
+    }
+
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k < a.v_count) {
         const int64_t v = a.v_begin + k;
         const int yi = (int)(v % a.ny);
         const int xi = (int)((v / a.ny) % a.nx);
@@ -291,15 +547,23 @@ __global__ void __launch_bounds__(128) k_bp_mixed(BpArgs a, MixedCtx m)
         const float P32[3] = {(float)(P[0] - m.ox), (float)(P[1] - m.oy), (float)P[2]};
         float accr = 0.f, acci = 0.f, cmpr = 0.f, cmpi = 0.f;
         for (int i = 0; i < np; i++) {
-            const double T[3] = {__ldg(a.tx + 3 * i), __ldg(a.tx + 3 * i + 1), __ldg(a.tx + 3 * i + 2)};
-            const double R[3] = {__ldg(a.rx + 3 * i), __ldg(a.rx + 3 * i + 1), __ldg(a.rx + 3 * i + 2)};
-            const float T32[3] = {(float)(T[0] - m.ox), (float)(T[1] - m.oy), (float)T[2]};
-            const float R32[3] = {(float)(R[0] - m.ox), (float)(R[1] - m.oy), (float)R[2]};
-            double r1t, r2t, r2r, r1r;
-            double Lida = solve_mixed(a.dem, m, T, P, T32, P32, n1f, n2f, a.W, r1t, r2t);
-            double Lvol = solve_mixed(a.dem, m, P, R, P32, R32, n2f, n1f, a.W, r2r, r1r);
-            // per-pulse legs: n1*r1Tx + n2*r2Tx + n2*r2Rx + n1*r1Rx
-            const double L = Lida + Lvol;
+            const double Tx[3] = {__ldg(a.tx + 3 * i), __ldg(a.tx + 3 * i + 1), __ldg(a.tx + 3 * i + 2)};
+            const double Rx[3] = {__ldg(a.rx + 3 * i), __ldg(a.rx + 3 * i + 1), __ldg(a.rx + 3 * i + 2)};
+            const float T32[3] = {(float)(Tx[0] - m.ox), (float)(Tx[1] - m.oy), (float)Tx[2]};
+            const float R32[3] = {(float)(Rx[0] - m.ox), (float)(Rx[1] - m.oy), (float)Rx[2]};
+            // per-pulse legs: n1*r1Tx + n2*r2Tx (Tx -> voxel) + n2*r2Rx + n1*r1Rx (voxel -> Rx);
+            // one solver body serves both legs
+            double L = 0.0;
+#pragma unroll 1
+            for (int leg = 0; leg < 2; leg++) {
+                // endpoints selected element-wise so they stay in registers
+                const double A[3] = {leg ? P[0] : Tx[0], leg ? P[1] : Tx[1], leg ? P[2] : Tx[2]};
+                const double B[3] = {leg ? Rx[0] : P[0], leg ? Rx[1] : P[1], leg ? Rx[2] : P[2]};
+                const float A32[3] = {leg ? P32[0] : T32[0], leg ? P32[1] : T32[1], leg ? P32[2] : T32[2]};
+                const float B32[3] = {leg ? R32[0] : P32[0], leg ? R32[1] : P32[1], leg ? R32[2] : P32[2]};
+                double dA, dB;
+                L += solve_mixed<WT>(a.dem, m, T, A, B, A32, B32, leg ? n2f : n1f, leg ? n1f : n2f, a.W, dA, dB);
+            }
             const float dL = (float)(L - __ldg(a.ref_L + i));
             // fast-time bin: integer anchor + FP32 offset
             const float t = __ldg(ref_bin_f + i) + dL * k_bin;
@@ -356,27 +620,85 @@ __global__ void __launch_bounds__(128) k_bp_mixed(BpArgs a, MixedCtx m)
         a.out[((int64_t)xi * a.ny + yi) * a.nz + zi] =
             make_double2((double)accr - (double)cmpr, (double)acci - (double)cmpi);
     }
+    if (ex.use_tile && !T.ok) drain_tile(&mbar);
 }
 
-cudaError_t launch_bp_mixed(const BpArgs& a, int legs, int fp16, cudaStream_t st)
+static MixedCtx mixed_ctx(const DemView& d, int pitch)
+{
+    MixedCtx m;
+    m.z32 = d.z32;
+    m.pitch = pitch;
+    m.nx = d.nx;
+    m.ny = d.ny;
+    m.stepx = (float)d.stepx;
+    m.stepy = (float)d.stepy;
+    m.ox = d.x0;
+    m.oy = d.y0;
+    return m;
+}
+
+// Crossing points of the mixed solver (FP32 scan and polish, FP64 final step) for n
+// (start, end) pairs: the data behind the mixed form's crossing-point error.
+__global__ void k_refraction_mixed(DemView d, MixedCtx m, const double* __restrict__ p1, const double* __restrict__ p2,
+                                   int64_t n, float na, float nb, int W, double* __restrict__ out)
+{
+    const Tile T{nullptr, 0, 0, false};
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const double A[3] = {p1[3 * k], p1[3 * k + 1], p1[3 * k + 2]};
+        const double B[3] = {p2[3 * k], p2[3 * k + 1], p2[3 * k + 2]};
+        const float A32[3] = {(float)(A[0] - m.ox), (float)(A[1] - m.oy), (float)A[2]};
+        const float B32[3] = {(float)(B[0] - m.ox), (float)(B[1] - m.oy), (float)B[2]};
+        double dA, dB, X[3];
+        solve_mixed<0>(d, m, T, A, B, A32, B32, na, nb, W, dA, dB, X);
+        out[3 * k] = X[0];
+        out[3 * k + 1] = X[1];
+        out[3 * k + 2] = X[2];
+    }
+}
+
+cudaError_t launch_refraction_mixed(const DemView& d, int pitch, const double* p1, const double* p2, int64_t n,
+                                    double n1, double n2, int W, double* out, cudaStream_t st)
+{
+    int64_t b = (n + 127) / 128;
+    int blocks = (int)(b < 1 ? 1 : (b > 148 * 64 ? 148 * 64 : b));
+    k_refraction_mixed<<<blocks, 128, 0, st>>>(d, mixed_ctx(d, pitch), p1, p2, n, (float)n1, (float)n2, W, out);
+    return cudaGetLastError();
+}
+
+template <int FP16, int WT>
+static void launch_w(const BpArgs& a, const MixedCtx& m, const MixedExtra& ex, const CUtensorMap& tmap, int blocks,
+                     cudaStream_t st)
+{
+    k_bp_mixed<FP16, WT><<<blocks, 128, 0, st>>>(a, m, ex, tmap);
+}
+
+template <int FP16>
+static void launch_fp(const BpArgs& a, const MixedCtx& m, const MixedExtra& ex, const CUtensorMap& tmap, int blocks,
+                      cudaStream_t st)
+{
+    switch (a.W) {
+    case 3: launch_w<FP16, 3>(a, m, ex, tmap, blocks, st); break;
+    case 6: launch_w<FP16, 6>(a, m, ex, tmap, blocks, st); break;
+    case 12: launch_w<FP16, 12>(a, m, ex, tmap, blocks, st); break;
+    default: launch_w<FP16, 0>(a, m, ex, tmap, blocks, st); break;
+    }
+}
+
+cudaError_t launch_bp_mixed(const BpArgs& a, const MixedLaunch& ml, int legs, int fp16, cudaStream_t st)
 {
     // the mean-over-pulses legs of the reference (proc_test_script.cpp:518-548) are served
     // by the FP64 form only
     if (legs == 0) return cudaErrorNotSupported;
-    MixedCtx m;
-    m.z32 = a.dem.z32;
-    m.nx = a.dem.nx;
-    m.ny = a.dem.ny;
-    m.stepx = (float)a.dem.stepx;
-    m.stepy = (float)a.dem.stepy;
-    m.ox = a.dem.x0;
-    m.oy = a.dem.y0;
+    MixedCtx m = mixed_ctx(a.dem, ml.pitch);
+    MixedExtra ex{ml.off_x, ml.off_y, ml.status, ml.tmap ? 1 : 0};
+    CUtensorMap tmap{};
+    if (ml.tmap) tmap = *reinterpret_cast<const CUtensorMap*>(ml.tmap);
     int64_t blocks64 = (a.v_count + 127) / 128;
     int blocks = (int)(blocks64 < 1 ? 1 : (blocks64 > (int64_t)1 << 30 ? (int64_t)1 << 30 : blocks64));
     if (fp16)
-        k_bp_mixed<1><<<blocks, 128, 0, st>>>(a, m);
+        launch_fp<1>(a, m, ex, tmap, blocks, st);
     else
-        k_bp_mixed<0><<<blocks, 128, 0, st>>>(a, m);
+        launch_fp<0>(a, m, ex, tmap, blocks, st);
     return cudaGetLastError();
 }
 

@@ -204,7 +204,7 @@ __global__ void __launch_bounds__(128) k_bp_plain(BpArgs a)
 __global__ void k_ref_ranges(DemView d, const double* __restrict__ tx, const double* __restrict__ rx, int np,
                              double cx, double cy, double cz, double n1, double n2, int W, double lambda,
                              double bin_per_m, double* __restrict__ ref_L, float* __restrict__ ref_phase,
-                             int* __restrict__ ref_bin_i, float* __restrict__ ref_bin_f)
+                             int* __restrict__ ref_bin_i, float* __restrict__ ref_bin_f, double* __restrict__ offsets)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += gridDim.x * blockDim.x) {
         const double T[3] = {tx[3 * i], tx[3 * i + 1], tx[3 * i + 2]};
@@ -226,6 +226,11 @@ __global__ void k_ref_ranges(DemView d, const double* __restrict__ tx, const dou
         double bf = floor(b);
         ref_bin_i[i] = (int)bf;
         ref_bin_f[i] = (float)(b - bf);
+        // crossing offsets from the centre (x, y) of both solves: DEM tile placement
+        offsets[4 * i] = ia[0] - cx;
+        offsets[4 * i + 1] = ia[1] - cy;
+        offsets[4 * i + 2] = vb[0] - cx;
+        offsets[4 * i + 3] = vb[1] - cy;
     }
 }
 
@@ -280,10 +285,10 @@ cudaError_t launch_bp_plain(const BpArgs& a, int solver, int legs, cudaStream_t 
 
 cudaError_t launch_ref_ranges(const DemView& d, const double* tx, const double* rx, int np, const double* center,
                               double n1, double n2, int W, double lambda, double bin_per_m, double* ref_L,
-                              float* ref_phase, int* ref_bin_i, float* ref_bin_f, cudaStream_t st)
+                              float* ref_phase, int* ref_bin_i, float* ref_bin_f, double* offsets, cudaStream_t st)
 {
     k_ref_ranges<<<grid_for(np, 64), 64, 0, st>>>(d, tx, rx, np, center[0], center[1], center[2], n1, n2, W, lambda,
-                                                  bin_per_m, ref_L, ref_phase, ref_bin_i, ref_bin_f);
+                                                  bin_per_m, ref_L, ref_phase, ref_bin_i, ref_bin_f, offsets);
     return cudaGetLastError();
 }
 

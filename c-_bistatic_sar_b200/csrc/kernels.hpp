@@ -71,10 +71,24 @@ struct BpArgs {
     const float* ref_bin_f; // np, ref_L * fs_eff / c - ref_bin_i
 };
 
+// DEM tile of the mixed kernel (nodes): TMA box dims.  The x extent is a multiple of
+// 4 floats so every tiled copy row is a multiple of 16 bytes.
+constexpr int kMixedTileI = 68;
+constexpr int kMixedTileJ = 64;
+
+struct MixedLaunch {
+    int pitch;            // row pitch (floats) of the FP32 DEM copy; a multiple of 4
+    const void* tmap;     // CUtensorMap of the FP32 DEM (box kMixedTileI x kMixedTileJ), or null
+    float off_x, off_y;   // mean crossing offset from the voxel, metres (tile centring)
+    int* status;          // device status word (1 = a tile copy timed out)
+};
+
 cudaError_t launch_bp_plain(const BpArgs& a, int solver, int legs, cudaStream_t st);
-cudaError_t launch_bp_mixed(const BpArgs& a, int legs, int fp16, cudaStream_t st);
+cudaError_t launch_refraction_mixed(const DemView& d, int pitch, const double* p1, const double* p2, int64_t n,
+                                    double n1, double n2, int W, double* out, cudaStream_t st);
+cudaError_t launch_bp_mixed(const BpArgs& a, const MixedLaunch& ml, int legs, int fp16, cudaStream_t st);
 cudaError_t launch_ref_ranges(const DemView& d, const double* tx, const double* rx, int np, const double* center,
                               double n1, double n2, int W, double lambda, double bin_per_m, double* ref_L,
-                              float* ref_phase, int* ref_bin_i, float* ref_bin_f, cudaStream_t st);
+                              float* ref_phase, int* ref_bin_i, float* ref_bin_f, double* offsets, cudaStream_t st);
 
 }  // namespace bsar

@@ -113,7 +113,8 @@ bsar_status bsar_dem_elevation(bsar_ctx* ctx, const bsar_dem* dem, const double*
                                double* z_out);
 
 /* calculateRefractionPoint, src/raw_data_processing.cpp:455-572, for n (start, end)
- * pairs (n x 3 each) with indices n1 (start side) and n2 (end side) -> points_out (n x 3). */
+ * pairs (n x 3 each) with indices n1 (start side) and n2 (end side) -> points_out (n x 3).
+ * fopts->precision BSAR_MIXED (Newton only) returns the mixed form's crossing points. */
 bsar_status bsar_refraction_points(bsar_ctx* ctx, const bsar_dem* dem, const double* p_start,
                                    const double* p_end, int64_t n, double n1, double n2,
                                    const bsar_fermat_opts* fopts, double* points_out);
