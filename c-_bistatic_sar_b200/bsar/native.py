@@ -14,7 +14,8 @@ from pathlib import Path
 import numpy as np
 
 PKG = Path(__file__).resolve().parent.parent          # c-_bistatic_sar_b200/
-LIB_PATH = PKG / "lib" / "libbsar.so"
+# BSAR_LIBRARY selects another build of the same library (e.g. an installed copy)
+LIB_PATH = Path(os.environ.get("BSAR_LIBRARY", PKG / "lib" / "libbsar.so"))
 CSRC = PKG / "csrc"
 
 _d = C.POINTER(C.c_double)

@@ -46,6 +46,7 @@ constexpr long kWaitSpins = 1L << 24;
 
 struct Facet32 {
     float x0, y0, dx, dy, z00, b, c, e;
+    float idx, idy;     // 1 / dx, 1 / dy
 };
 
 struct MixedCtx {
@@ -53,7 +54,9 @@ struct MixedCtx {
     int pitch;
     int nx, ny;
     float stepx, stepy;             // uniform node spacing
+    float istepx, istepy;           // 1 / spacing
     double ox, oy;                  // origin of the FP32 frame (first DEM node)
+    double idx64, idy64;            // 1 / spacing, FP64
 };
 
 // A DEM tile in shared memory: node (i, j) at s[(j - j0) * TI + (i - i0)].
@@ -68,7 +71,7 @@ __device__ __forceinline__ float zf(const MixedCtx& m, int i, int j) { return __
 // FP32 bilinear height (clamped to the DEM) for the flat-interface start.
 __device__ __forceinline__ float height32(const MixedCtx& m, float x, float y)
 {
-    float fx = x / m.stepx, fy = y / m.stepy;
+    float fx = x * m.istepx, fy = y * m.istepy;
     int i = min(max((int)floorf(fx), 0), m.nx - 2);
     int j = min(max((int)floorf(fy), 0), m.ny - 2);
     float u = fminf(fmaxf(fx - (float)i, 0.f), 1.f), v = fminf(fmaxf(fy - (float)j, 0.f), 1.f);
@@ -81,40 +84,42 @@ __device__ __forceinline__ bool facet_step32(const Facet32& F, const float A[3],
 {
     float x = fmaf(u, F.dx, F.x0), y = fmaf(v, F.dy, F.y0);
     float h = F.z00 + F.b * u + F.c * v + F.e * u * v;
-    float idx_ = 1.0f / F.dx, idy = 1.0f / F.dy;
+    const float idx_ = F.idx, idy = F.idy;
     float zx = (F.b + F.e * v) * idx_;
     float zy = (F.c + F.e * u) * idy;
-    float zxy = F.e * idx_ * idy;
     float r1x = x - A[0], r1y = y - A[1], r1z = h - A[2];
     float r2x = x - B[0], r2y = y - B[1], r2z = h - B[2];
     float q1 = r1x * r1x + r1y * r1y + r1z * r1z;
     float q2 = r2x * r2x + r2y * r2y + r2z * r2z;
     float s1 = rsqrtf(q1), s2 = rsqrtf(q2);
     float g1 = na * s1, g2 = nb * s2;
-    float iq1 = s1 * s1, iq2 = s2 * s2;
     float a1x = r1x + r1z * zx, a1y = r1y + r1z * zy;
     float a2x = r2x + r2z * zx, a2y = r2y + r2z * zy;
     float gx = g1 * a1x + g2 * a2x;
     float gy = g1 * a1y + g2 * a2y;
+    // active set first: a corner the gradient pushes outward of on both axes is this
+    // facet's minimum, and the Hessian is not needed
+    bool au = (u <= 0.0f && gx > 0.0f) || (u >= 1.0f && gx < 0.0f);
+    bool av = (v <= 0.0f && gy > 0.0f) || (v >= 1.0f && gy < 0.0f);
+    if (au && av) return false;
+    float zxy = F.e * idx_ * idy;
+    float iq1 = s1 * s1, iq2 = s2 * s2;
     float txx = 1.0f + zx * zx, tyy = 1.0f + zy * zy, txy = zx * zy;
     float hxx = g1 * (txx - a1x * a1x * iq1) + g2 * (txx - a2x * a2x * iq2);
     float hyy = g1 * (tyy - a1y * a1y * iq1) + g2 * (tyy - a2y * a2y * iq2);
     float hxy = g1 * (txy - a1x * a1y * iq1) + g2 * (txy - a2x * a2y * iq2) + (g1 * r1z + g2 * r2z) * zxy;
-    bool au = (u <= 0.0f && gx > 0.0f) || (u >= 1.0f && gx < 0.0f);
-    bool av = (v <= 0.0f && gy > 0.0f) || (v >= 1.0f && gy < 0.0f);
-    if (au && av) return false;
-    float igs = 1.0f / (g1 + g2);
+    float igs = __frcp_rn(g1 + g2);
     float su, sv;
     if (au) {
         su = 0.0f;
-        sv = (hyy > 0.0f) ? -gy / hyy : -gy * igs;
+        sv = (hyy > 0.0f) ? -gy * __frcp_rn(hyy) : -gy * igs;
     } else if (av) {
         sv = 0.0f;
-        su = (hxx > 0.0f) ? -gx / hxx : -gx * igs;
+        su = (hxx > 0.0f) ? -gx * __frcp_rn(hxx) : -gx * igs;
     } else {
         float det = hxx * hyy - hxy * hxy;
         if (det > 0.0f && hxx > 0.0f) {
-            float idet = 1.0f / det;
+            float idet = __frcp_rn(det);
             su = -(hyy * gx - hxy * gy) * idet;
             sv = -(hxx * gy - hxy * gx) * idet;
         } else {
@@ -143,14 +148,13 @@ __device__ __forceinline__ float facet_eval32(const Facet32& F, const float A[3]
 // result and its two leg lengths (|X-A|, |X-B|).
 __device__ __forceinline__ double final_step64(const DemView& d, int fi, int fj, const double A[3], const double B[3],
                                                double na, double nb, double u, double v, double& dA, double& dB,
-                                               double* X)
+                                               double* X, double idx_, double idy)
 {
     Facet64 F;
     facet_load(d, fi, fj, F);
     {
         double x = F.x0 + u * F.dx, y = F.y0 + v * F.dy;
         double h = F.z00 + F.b * u + F.c * v + F.e * u * v;
-        double idx_ = 1.0 / F.dx, idy = 1.0 / F.dy;
         double zx = (F.b + F.e * v) * idx_;
         double zy = (F.c + F.e * u) * idy;
         double zxy = F.e * idx_ * idy;
@@ -172,24 +176,25 @@ __device__ __forceinline__ double final_step64(const DemView& d, int fi, int fj,
         bool au = (u <= 0.0 && gx > 0.0) || (u >= 1.0 && gx < 0.0);
         bool av = (v <= 0.0 && gy > 0.0) || (v >= 1.0 && gy < 0.0);
         if (!(au && av)) {
-            double igs = 1.0 / (g1 + g2);
+            // one division: the reciprocal of the pivot the taken branch needs
+            double det = hxx * hyy - hxy * hxy;
+            const bool newton = !au && !av && det > 0.0 && hxx > 0.0;
+            const bool axis = (au && hyy > 0.0) || (av && !au && hxx > 0.0);
+            const double piv = newton ? det : (axis ? (au ? hyy : hxx) : g1 + g2);
+            const double ip = 1.0 / piv;
             double su, sv;
-            if (au) {
+            if (newton) {
+                su = -(hyy * gx - hxy * gy) * ip;
+                sv = -(hxx * gy - hxy * gx) * ip;
+            } else if (au) {
                 su = 0.0;
-                sv = (hyy > 0.0) ? -gy / hyy : -gy * igs;
+                sv = -gy * ip;
             } else if (av) {
                 sv = 0.0;
-                su = (hxx > 0.0) ? -gx / hxx : -gx * igs;
+                su = -gx * ip;
             } else {
-                double det = hxx * hyy - hxy * hxy;
-                if (det > 0.0 && hxx > 0.0) {
-                    double idet = 1.0 / det;
-                    su = -(hyy * gx - hxy * gy) * idet;
-                    sv = -(hxx * gy - hxy * gx) * idet;
-                } else {
-                    su = -gx * igs;
-                    sv = -gy * igs;
-                }
+                su = -gx * ip;
+                sv = -gy * ip;
             }
             u = clamp01(u + su * idx_);
             v = clamp01(v + sv * idy);
@@ -222,17 +227,10 @@ __device__ __forceinline__ double node_l64(const DemView& d, int i, int j, const
     return __dadd_rn(__dmul_rn(na, __dsqrt_rn(q1)), __dmul_rn(nb, __dsqrt_rn(q2)));
 }
 
-// Scaled FP32 node path |N-A| + rb |N-B| (rb = nb / na; ranking is scale-free).
-__device__ __forceinline__ float node_l32(float z, float sxa, float sya, float sxb, float syb, float Az, float Bz,
-                                          float rb)
-{
-    float dza = z - Az, dzb = z - Bz;
-    float qa = fmaf(dza, dza, sxa + sya);
-    float qb = fmaf(dzb, dzb, sxb + syb);
-    return fmaf(rb, qb * rsqrtf(qb), qa * rsqrtf(qa));
-}
+// Node ranking values.  G is the voxel-side endpoint of the path (index ng), E the
+// other one (index ne); the scans rank L' = re |N-E| + |N-G| = L / ng with re = ne / ng.
 
-// Branch-free ranking update: best value / index and runner-up value.
+// Branch-free ranking update: best value / position and runner-up value.
 __device__ __forceinline__ void rank(float L, int i, int j, float& v1, float& v2, int& bi, int& bj)
 {
     v2 = fminf(v2, fmaxf(v1, L));
@@ -242,73 +240,120 @@ __device__ __forceinline__ void rank(float L, int i, int j, float& v1, float& v2
     bj = p ? j : bj;
 }
 
-// Node scan over [ia, ib] x [ja, jb] (clamped window), generic width; z from the tile
-// when `in_tile`, else from global memory.
 struct Rank {
     float v1, v2;
     int bi, bj;
 };
 
+// Generic node scan over [ia, ib] x [ja, jb]: both legs per node, z from the tile when
+// `in_tile`, else from global memory.
 __device__ __noinline__ Rank scan_generic(const MixedCtx m, const float* ts, int ti0, int tj0, bool in_tile, int ia,
-                                          int ib, int ja, int jb, float ax, float ay, float az, float bx, float by,
-                                          float bz, float rb, Rank r)
+                                          int ib, int ja, int jb, float ex, float ey, float ez, float gx, float gy,
+                                          float gz, float re, Rank r)
 {
     for (int i = ia; i <= ib; i++) {
         float xi = (float)i * m.stepx;
-        float dxa = xi - ax, dxb = xi - bx;
-        float sxa = dxa * dxa, sxb = dxb * dxb;
+        float dxe = xi - ex, dxg = xi - gx;
+        float sxe = dxe * dxe, sxg = dxg * dxg;
         for (int j = ja; j <= jb; j++) {
             float yj = (float)j * m.stepy;
-            float dya = yj - ay, dyb = yj - by;
+            float dye = yj - ey, dyg = yj - gy;
             float z = in_tile ? ts[(j - tj0) * TI + (i - ti0)] : zf(m, i, j);
-            rank(node_l32(z, sxa, dya * dya, sxb, dyb * dyb, az, bz, rb), i, j, r.v1, r.v2, r.bi, r.bj);
+            float dze = z - ez, dzg = z - gz;
+            float qe = fmaf(dze, dze, fmaf(dye, dye, sxe));
+            float qg = fmaf(dzg, dzg, fmaf(dyg, dyg, sxg));
+            rank(fmaf(re, qe * rsqrtf(qe), qg * rsqrtf(qg)), i, j, r.v1, r.v2, r.bi, r.bj);
         }
     }
     return r;
 }
 
-// Full (2W+1)^2 window inside the DEM and inside the tile: per-column terms in registers,
-// fully unrolled columns, tile reads at compile-time offsets.
-template <int W>
-__device__ __forceinline__ void scan_tile(const MixedCtx& m, const Tile& T, int is, int js, const float A[3],
-                                          const float B[3], float rb, float& v1, float& v2, int& bi, int& bj)
+// Per-warp table of the E-leg term re |N-E| over the union of the 32 lanes' windows (all
+// lanes solve the same pulse, so this leg does not depend on the voxel).  Lane l fills
+// column j0 + l.  Warp-uniform; `ok` is false when the union does not fit.
+constexpr int TBJ = 32;
+constexpr int TBI = 24;
+
+struct AirTable {
+    float* t;
+    int i0, j0;
+    bool ok;
+};
+
+__device__ __forceinline__ AirTable build_air_table(const MixedCtx& m, const Tile& T, float* buf, int is, int js, int W,
+                                                    float ex, float ey, float ez, float re)
 {
-    constexpr int NJ = 2 * W + 1;
-    float sya[NJ], syb[NJ];
-#pragma unroll
-    for (int c = 0; c < NJ; c++) {
-        float yj = (float)(js - W + c) * m.stepy;
-        float dya = yj - A[1], dyb = yj - B[1];
-        sya[c] = dya * dya;
-        syb[c] = dyb * dyb;
+    const unsigned full = 0xffffffffu;
+    int i0 = max(__reduce_min_sync(full, is) - W, 0), i1 = min(__reduce_max_sync(full, is) + W, m.nx - 1);
+    int j0 = max(__reduce_min_sync(full, js) - W, 0), j1 = min(__reduce_max_sync(full, js) + W, m.ny - 1);
+    AirTable A{buf, i0, j0, false};
+    __syncwarp();                       // readers of the previous table are done
+    if (i1 - i0 + 1 > TBI || j1 - j0 + 1 > TBJ) return A;
+    const int lane = threadIdx.x & 31;
+    const int j = j0 + lane;
+    const bool in_tile = T.ok && i0 >= T.i0 && i1 < T.i0 + TI && j0 >= T.j0 && j1 < T.j0 + TJ;
+    if (j <= j1) {
+        float dy = (float)j * m.stepy - ey;
+        float sy = dy * dy;
+        for (int i = i0; i <= i1; i++) {
+            float z = in_tile ? T.s[(j - T.j0) * TI + (i - T.i0)] : zf(m, i, j);
+            float dx = (float)i * m.stepx - ex, dz = z - ez;
+            float q = fmaf(dz, dz, fmaf(dx, dx, sy));
+            buf[(i - i0) * TBJ + lane] = re * (q * rsqrtf(q));
+        }
     }
-    const float* col0 = T.s + (js - W - T.j0) * TI - T.i0;
-#pragma unroll 1
-    for (int i = is - W; i <= is + W; i++) {
-        float xi = (float)i * m.stepx;
-        float dxa = xi - A[0], dxb = xi - B[0];
-        float sxa = dxa * dxa, sxb = dxb * dxb;
-        const float* zc = col0 + i;
-#pragma unroll
-        for (int c = 0; c < NJ; c++)
-            rank(node_l32(zc[c * TI], sxa, sya[c], sxb, syb[c], A[2], B[2], rb), i, js - W + c, v1, v2, bi, bj);
-    }
+    __syncwarp();
+    A.ok = true;
+    return A;
 }
 
+// Full (2W+1)^2 window inside the DEM, the tile and the warp table: the E leg from the
+// table, the G leg per node, columns unrolled with compile-time offsets.
 template <int W>
-__device__ __forceinline__ void node_scan(const MixedCtx& m, const Tile& T, int is, int js, int Wr, const float A[3],
-                                          const float B[3], float rb, float& v1, float& v2, int& bi, int& bj)
+__device__ __forceinline__ void scan_table(const MixedCtx& m, const Tile& T, const AirTable& AT, int is, int js,
+                                           float gx, float gy, float gz, float& v1, float& v2, int& bi, int& bj)
+{
+    constexpr int NJ = 2 * W + 1;
+    float syg[NJ];
+#pragma unroll
+    for (int c = 0; c < NJ; c++) {
+        float dy = (float)(js - W + c) * m.stepy - gy;
+        syg[c] = dy * dy;
+    }
+    const float* zc0 = T.s + (js - W - T.j0) * TI - T.i0;
+    const float* ac0 = AT.t + (js - W - AT.j0) - AT.i0 * TBJ;
+    int bc = bj - (js - W);
+#pragma unroll 1
+    for (int i = is - W; i <= is + W; i++) {
+        float dx = (float)i * m.stepx - gx;
+        float sxg = dx * dx;
+        const float* zc = zc0 + i;
+        const float* ac = ac0 + i * TBJ;
+#pragma unroll
+        for (int c = 0; c < NJ; c++) {
+            float dz = zc[c * TI] - gz;
+            float q = fmaf(dz, dz, sxg + syg[c]);
+            rank(fmaf(q, rsqrtf(q), ac[c]), i, c, v1, v2, bi, bc);
+        }
+    }
+    bj = js - W + bc;
+}
+
+template <int W, bool TABLE>
+__device__ __forceinline__ void node_scan(const MixedCtx& m, const Tile& T, const AirTable& AT, int is, int js, int Wr,
+                                          const float E[3], const float G[3], float re, float& v1, float& v2, int& bi,
+                                          int& bj)
 {
     const int ia = max(is - Wr, 0), ib = min(is + Wr, m.nx - 1);
     const int ja = max(js - Wr, 0), jb = min(js + Wr, m.ny - 1);
     const bool in_tile = T.ok && ia >= T.i0 && ib < T.i0 + TI && ja >= T.j0 && jb < T.j0 + TJ;
-    if constexpr (W > 0) {
-        if (in_tile && Wr == W && ia == is - W && ib == is + W && ja == js - W && jb == js + W) {
-            scan_tile<W>(m, T, is, js, A, B, rb, v1, v2, bi, bj);
+    if constexpr (W > 0 && TABLE) {
+        if (AT.ok && in_tile && Wr == W && ia == is - W && ib == is + W && ja == js - W && jb == js + W) {
+            scan_table<W>(m, T, AT, is, js, G[0], G[1], G[2], v1, v2, bi, bj);
             return;
         }
     }
-    Rank r = scan_generic(m, T.s, T.i0, T.j0, in_tile, ia, ib, ja, jb, A[0], A[1], A[2], B[0], B[1], B[2], rb,
+    Rank r = scan_generic(m, T.s, T.i0, T.j0, in_tile, ia, ib, ja, jb, E[0], E[1], E[2], G[0], G[1], G[2], re,
                           Rank{v1, v2, bi, bj});
     v1 = r.v1;
     v2 = r.v2;
@@ -316,11 +361,11 @@ __device__ __forceinline__ void node_scan(const MixedCtx& m, const Tile& T, int 
     bj = r.bj;
 }
 
-// FP64 re-ranking of the nodes within the FP32 ambiguity band, in the FP64 solver's
-// order (i-major, j-minor, strict <).
+// FP64 re-ranking of the nodes within the FP32 ambiguity band, with the FP64 solver's
+// arithmetic and order (i-major, j-minor, strict <).
 __device__ __noinline__ int2 rerank64(const DemView d, const MixedCtx m, const float* ts, int ti0, int tj0, bool tok,
-                                      int is, int js, int Wr, float ax, float ay, float az, float bx, float by,
-                                      float bz, float rb, float limit, double Ax, double Ay, double Az, double Bx,
+                                      int is, int js, int Wr, float ex, float ey, float ez, float gx, float gy,
+                                      float gz, float re, float limit, double Ax, double Ay, double Az, double Bx,
                                       double By, double Bz, double na, double nb, int2 best_ij)
 {
     const int ia = max(is - Wr, 0), ib = min(is + Wr, m.nx - 1);
@@ -330,13 +375,15 @@ __device__ __noinline__ int2 rerank64(const DemView d, const MixedCtx m, const f
     double best = INFINITY;
     for (int i = ia; i <= ib; i++) {
         float xi = (float)i * m.stepx;
-        float dxa = xi - ax, dxb = xi - bx;
-        float sxa = dxa * dxa, sxb = dxb * dxb;
+        float dxe = xi - ex, dxg = xi - gx;
         for (int j = ja; j <= jb; j++) {
             float yj = (float)j * m.stepy;
-            float dya = yj - ay, dyb = yj - by;
+            float dye = yj - ey, dyg = yj - gy;
             float z = in_tile ? ts[(j - tj0) * TI + (i - ti0)] : zf(m, i, j);
-            if (node_l32(z, sxa, dya * dya, sxb, dyb * dyb, az, bz, rb) <= limit) {
+            float dze = z - ez, dzg = z - gz;
+            float qe = dxe * dxe + dye * dye + dze * dze;
+            float qg = dxg * dxg + dyg * dyg + dzg * dzg;
+            if (re * sqrtf(qe) + sqrtf(qg) <= limit) {
                 double L = node_l64(d, i, j, A, B, na, nb);
                 if (L < best) {
                     best = L;
@@ -364,13 +411,15 @@ __device__ __noinline__ int2 start_node64(const DemView d, double Ax, double Ay,
     return make_int2(nearest_node(d.x0, d.stepx, d.nx, sx), nearest_node(d.y0, d.stepy, d.ny, sy));
 }
 
-// Mixed-precision crossing solve A (index na) -> B (index nb).  A32/B32: the endpoints in
-// the FP32 frame.  Returns the FP64 optical path; dA, dB: FP64 leg lengths; X (optional):
-// the crossing point.
-template <int WT>
-__device__ __forceinline__ double solve_mixed(const DemView& d, const MixedCtx& m, const Tile& T, const double A[3],
-                                              const double B[3], const float A32[3], const float B32[3], float na,
-                                              float nb, int W, double& dA, double& dB, double* X = nullptr)
+// Mixed-precision crossing solve A (index na) -> B (index nb); the voxel-side endpoint G
+// is B when g_is_b, else A.  A32/B32: the endpoints in the FP32 frame.  With TABLE the
+// warp builds and uses the shared E-leg table (all 32 lanes must call together).
+// Returns the FP64 optical path; dA, dB: FP64 leg lengths; X (optional): the crossing.
+template <int WT, bool TABLE>
+__device__ __forceinline__ double solve_mixed(const DemView& d, const MixedCtx& m, const Tile& T, float* table_buf,
+                                              const double A[3], const double B[3], const float A32[3],
+                                              const float B32[3], float na, float nb, bool g_is_b, int W, double& dA,
+                                              double& dB, double* X = nullptr)
 {
     // 1. flat-interface start (FP32)
     const bool lower_b = nb >= na;
@@ -379,26 +428,28 @@ __device__ __forceinline__ double solve_mixed(const DemView& d, const MixedCtx& 
     const float nl = lower_b ? nb : na, nu = lower_b ? na : nb;
     float h0 = height32(m, Lp[0], Lp[1]);
     float hx = Lp[0] - Up[0], hy = Lp[1] - Up[1];
-    float D = sqrtf(hx * hx + hy * hy);
+    const float D2 = hx * hx + hy * hy;
+    float D = D2 * rsqrtf(D2);
     float sx = Lp[0], sy = Lp[1];
     if (D >= 1e-6f) {
         float ha = fabsf(Up[2] - h0), hb = fabsf(Lp[2] - h0);
-        float s = fminf(fmaxf(D * ha / (ha + hb + 1e-30f), 0.f), D);
+        float s = fminf(fmaxf(__fdividef(D * ha, ha + hb + 1e-30f), 0.f), D);
 #pragma unroll
         for (int it = 0; it < kFlatIters; it++) {
             float q1 = s * s + ha * ha, r = D - s, q2 = r * r + hb * hb;
             float i1 = rsqrtf(q1), i2 = rsqrtf(q2);
             float g = nu * s * i1 - nl * r * i2;
             float gp = nu * ha * ha * i1 * i1 * i1 + nl * hb * hb * i2 * i2 * i2;
-            if (gp > 0.f) s = fminf(fmaxf(s - g / gp, 0.f), D);
+            if (gp > 0.f) s = fminf(fmaxf(s - __fdividef(g, gp), 0.f), D);
         }
-        sx = Up[0] + hx * (s / D);
-        sy = Up[1] + hy * (s / D);
+        const float t = __fdividef(s, D);
+        sx = Up[0] + hx * t;
+        sy = Up[1] + hy * t;
     }
-    // 2. node scan (FP32, scaled by 1/na), FP64 re-rank of near ties.  The window centre is
-    //    the node nearest the start; a start within rounding distance of a cell boundary
-    //    is redone in FP64 so both forms scan the same window.
-    const float fx = sx / m.stepx, fy = sy / m.stepy;
+    // 2. node scan (FP32, L / ng), FP64 re-rank of near ties.  The window centre is the
+    //    node nearest the start; a start within rounding distance of a cell boundary is
+    //    redone in FP64 so both forms scan the same window.
+    const float fx = sx * m.istepx, fy = sy * m.istepy;
     int is = min(max(__float2int_rn(fx), 0), m.nx - 1);
     int js = min(max(__float2int_rn(fy), 0), m.ny - 1);
     if (fabsf(fabsf(fx - rintf(fx)) - 0.5f) < kStartBand || fabsf(fabsf(fy - rintf(fy)) - 0.5f) < kStartBand) {
@@ -406,19 +457,32 @@ __device__ __forceinline__ double solve_mixed(const DemView& d, const MixedCtx& 
         is = s64.x;
         js = s64.y;
     }
-    const float rb = nb / na;
+    const float* E = g_is_b ? A32 : B32;
+    const float* G = g_is_b ? B32 : A32;
+    const float ng = g_is_b ? nb : na;
+    const float re = (g_is_b ? na : nb) / ng;
+    AirTable AT{table_buf, 0, 0, false};
+    if constexpr (TABLE) AT = build_air_table(m, T, table_buf, is, js, W, E[0], E[1], E[2], re);
     float v1 = INFINITY, v2 = INFINITY;
     int bi = is, bj = js;
-    node_scan<WT>(m, T, is, js, W, A32, B32, rb, v1, v2, bi, bj);
-    const float tie = kTieM / na;
+    node_scan<WT, TABLE>(m, T, AT, is, js, W, E, G, re, v1, v2, bi, bj);
+    const float tie = kTieM / ng;
     if (!(v2 - v1 >= tie)) {
-        const int2 b = rerank64(d, m, T.s, T.i0, T.j0, T.ok, is, js, W, A32[0], A32[1], A32[2], B32[0], B32[1], B32[2],
-                                rb, v1 + tie, A[0], A[1], A[2], B[0], B[1], B[2], (double)na, (double)nb,
+        const int2 b = rerank64(d, m, T.s, T.i0, T.j0, T.ok, is, js, W, E[0], E[1], E[2], G[0], G[1], G[2], re,
+                                v1 + tie, A[0], A[1], A[2], B[0], B[1], B[2], (double)na, (double)nb,
                                 make_int2(bi, bj));
         bi = b.x;
         bj = b.y;
     }
     // 3. polish the facets around the best node (FP32)
+    float Lnode;
+    {
+        float xn = (float)bi * m.stepx, yn = (float)bj * m.stepy, zn = zf(m, bi, bj);
+        float r1x = xn - A32[0], r1y = yn - A32[1], r1z = zn - A32[2];
+        float r2x = xn - B32[0], r2y = yn - B32[1], r2z = zn - B32[2];
+        float q1 = r1x * r1x + r1y * r1y + r1z * r1z, q2 = r2x * r2x + r2y * r2y + r2z * r2z;
+        Lnode = na * (q1 * rsqrtf(q1)) + nb * (q2 * rsqrtf(q2));
+    }
     int bfi = min(bi, m.nx - 2), bfj = min(bj, m.ny - 2);     // fallback facet
     float bestF = INFINITY, bu = (float)(bi - bfi), bv = (float)(bj - bfj);
 #pragma unroll 1
@@ -430,16 +494,22 @@ __device__ __forceinline__ double solve_mixed(const DemView& d, const MixedCtx& 
         F.y0 = (float)fj * m.stepy;
         F.dx = m.stepx;
         F.dy = m.stepy;
+        F.idx = m.istepx;
+        F.idy = m.istepy;
         float z00 = zf(m, fi, fj), z01 = zf(m, fi + 1, fj), z10 = zf(m, fi, fj + 1), z11 = zf(m, fi + 1, fj + 1);
         F.z00 = z00;
         F.b = z01 - z00;
         F.c = z10 - z00;
         F.e = z11 - z01 - z10 + z00;
         float u = (float)(bi - fi), v = (float)(bj - fj);
+        bool moved = false;
 #pragma unroll 1
-        for (int it = 0; it < kPolishIters; it++)
+        for (int it = 0; it < kPolishIters; it++) {
             if (!facet_step32(F, A32, B32, na, nb, u, v)) break;
-        float L = facet_eval32(F, A32, B32, na, nb, u, v);
+            moved = true;
+        }
+        // a facet whose corner is already its minimum keeps the best node's path
+        float L = moved ? facet_eval32(F, A32, B32, na, nb, u, v) : Lnode;
         if (L < bestF) {
             bestF = L;
             bu = u;
@@ -449,7 +519,8 @@ __device__ __forceinline__ double solve_mixed(const DemView& d, const MixedCtx& 
         }
     }
     // 4. FP64 final step
-    return final_step64(d, bfi, bfj, A, B, (double)na, (double)nb, (double)bu, (double)bv, dA, dB, X);
+    return final_step64(d, bfi, bfj, A, B, (double)na, (double)nb, (double)bu, (double)bv, dA, dB, X, m.idx64,
+                        m.idy64);
 }
 
 // ------------------------------- TMA tile staging -----------------------------------
@@ -510,11 +581,13 @@ struct MixedExtra {
 }  // namespace
 
 template <int FP16, int WT>
-__global__ void __launch_bounds__(128, 4) k_bp_mixed(BpArgs a, MixedCtx m, MixedExtra ex,
+__global__ void __launch_bounds__(128, 5) k_bp_mixed(BpArgs a, MixedCtx m, MixedExtra ex,
                                                   const __grid_constant__ CUtensorMap tmap)
 {
     __shared__ alignas(128) float tile_s[TI * TJ];
+    __shared__ alignas(16) float air_s[4][TBI * TBJ];     // one E-leg table per warp
     __shared__ alignas(8) uint64_t mbar;
+    float* table_buf = air_s[threadIdx.x >> 5];
     const int* __restrict__ ref_bin_i = a.ref_bin_i;
     const float* __restrict__ ref_bin_f = a.ref_bin_f;
     const int np = a.np;
@@ -537,8 +610,11 @@ __global__ void __launch_bounds__(128, 4) k_bp_mixed(BpArgs a, MixedCtx m, Mixed
         T.ok = stage_tile(&tmap, tile_s, &mbar, T.i0, T.j0, ex.status);
     }
 
-    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (k < a.v_count) {
+    // every lane walks the pulses (the warp tables need the full warp); lanes past the
+    // end of the grid repeat the last voxel and do not store it
+    const int64_t kk = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    {
+        const int64_t k = kk < a.v_count ? kk : a.v_count - 1;
         const int64_t v = a.v_begin + k;
         const int yi = (int)(v % a.ny);
         const int xi = (int)((v / a.ny) % a.nx);
@@ -562,7 +638,8 @@ __global__ void __launch_bounds__(128, 4) k_bp_mixed(BpArgs a, MixedCtx m, Mixed
                 const float A32[3] = {leg ? P32[0] : T32[0], leg ? P32[1] : T32[1], leg ? P32[2] : T32[2]};
                 const float B32[3] = {leg ? R32[0] : P32[0], leg ? R32[1] : P32[1], leg ? R32[2] : P32[2]};
                 double dA, dB;
-                L += solve_mixed<WT>(a.dem, m, T, A, B, A32, B32, leg ? n2f : n1f, leg ? n1f : n2f, a.W, dA, dB);
+                L += solve_mixed<WT, true>(a.dem, m, T, table_buf, A, B, A32, B32, leg ? n2f : n1f, leg ? n1f : n2f,
+                                           leg == 0, a.W, dA, dB);
             }
             const float dL = (float)(L - __ldg(a.ref_L + i));
             // fast-time bin: integer anchor + FP32 offset
@@ -617,8 +694,9 @@ __global__ void __launch_bounds__(128, 4) k_bp_mixed(BpArgs a, MixedCtx m, Mixed
                 acci = tt;
             }
         }
-        a.out[((int64_t)xi * a.ny + yi) * a.nz + zi] =
-            make_double2((double)accr - (double)cmpr, (double)acci - (double)cmpi);
+        if (kk < a.v_count)
+            a.out[((int64_t)xi * a.ny + yi) * a.nz + zi] =
+                make_double2((double)accr - (double)cmpr, (double)acci - (double)cmpi);
     }
     if (ex.use_tile && !T.ok) drain_tile(&mbar);
 }
@@ -632,8 +710,12 @@ static MixedCtx mixed_ctx(const DemView& d, int pitch)
     m.ny = d.ny;
     m.stepx = (float)d.stepx;
     m.stepy = (float)d.stepy;
+    m.istepx = (float)(1.0 / d.stepx);
+    m.istepy = (float)(1.0 / d.stepy);
     m.ox = d.x0;
     m.oy = d.y0;
+    m.idx64 = 1.0 / d.stepx;
+    m.idy64 = 1.0 / d.stepy;
     return m;
 }
 
@@ -649,7 +731,7 @@ __global__ void k_refraction_mixed(DemView d, MixedCtx m, const double* __restri
         const float A32[3] = {(float)(A[0] - m.ox), (float)(A[1] - m.oy), (float)A[2]};
         const float B32[3] = {(float)(B[0] - m.ox), (float)(B[1] - m.oy), (float)B[2]};
         double dA, dB, X[3];
-        solve_mixed<0>(d, m, T, A, B, A32, B32, na, nb, W, dA, dB, X);
+        solve_mixed<0, false>(d, m, T, nullptr, A, B, A32, B32, na, nb, true, W, dA, dB, X);
         out[3 * k] = X[0];
         out[3 * k + 1] = X[1];
         out[3 * k + 2] = X[2];
