@@ -406,11 +406,14 @@ static void compress_scene(bsar_ctx* ctx, Scene* s, int precision)
     a.out16 = precision == BSAR_MIXED_FP16 ? rb.data->as<__half2>() : nullptr;
     a.scale16 = rb.scale ? rb.scale->as<float>() : nullptr;
     if (s->kind == BSAR_SAMPLES_COMPRESSED) {
-        if (precision == BSAR_FP64) {
+        // already range-compressed: upsampling only (splineInterpolation)
+        if (precision == BSAR_FP64)
             launched(ctx, launch_spline(a.in, s->ns, s->np, s->upsample, a.out64, ctx->stream), "spline");
-            return;
-        }
-        // identity spectrum: one FFT round trip, then the upsampling epilogue
+        else
+            launched(ctx, launch_upsample_store(a.in, s->ns, s->np, s->upsample, precision, a.out32, a.out16, a.scale16,
+                                                ctx->stream),
+                     "upsample");
+        return;
     }
     if (s->ns > max_fft_len(a.real_bytes))
         fail(BSAR_ERR_UNSUPPORTED, "pulse length %lld exceeds the single-CTA FFT (%lld for this precision)",
@@ -421,12 +424,7 @@ static void compress_scene(bsar_ctx* ctx, Scene* s, int precision)
         // the reference's spectrum once per scene and precision (the reference recomputes
         // it for every pulse, src/fft_utils.cpp:81-82)
         spec = dev_alloc(ctx, (size_t)a.P * (a.real_bytes == 8 ? sizeof(double2) : sizeof(float2)));
-        std::vector<double> ref = s->reference;
-        if (s->kind == BSAR_SAMPLES_COMPRESSED) {
-            // delta reference: its spectrum is all ones, the filter is the identity
-            ref.assign(2 * (size_t)s->ns, 0.0);
-            ref[0] = 1.0;
-        }
+        const std::vector<double>& ref = s->reference;
         auto dref = dev_upload(ctx, ref.data(), sizeof(double) * ref.size());
         launched(ctx, launch_ref_spectrum(dref->as<double2>(), (int)s->ns, a.P, a.logP, a.tw, 1, spec->p,
                                           a.real_bytes, ctx->stream),
@@ -714,7 +712,8 @@ bsar_status bsar_scene_upload(bsar_ctx* ctx, const bsar_scene_desc* desc, bsar_s
         const bsar_scene_desc& s = *desc;
         if (s.n_pulses < 1 || !s.tx || !s.rx) fail(BSAR_ERR_INVALID_ARG, "no pulses / trajectories");
         if (s.n_samples < 2 || !s.samples) fail(BSAR_ERR_INVALID_ARG, "no samples");
-        if (!is_pow2(s.n_samples)) fail(BSAR_ERR_INVALID_ARG, "n_samples must be a power of two");
+        if (s.samples_kind == BSAR_SAMPLES_RAW && !is_pow2(s.n_samples))
+            fail(BSAR_ERR_INVALID_ARG, "raw pulses must have a power-of-two length");
         if (s.upsample < 1 || s.upsample > 64) fail(BSAR_ERR_INVALID_ARG, "upsample factor out of range");
         if (s.samples_kind != BSAR_SAMPLES_RAW && s.samples_kind != BSAR_SAMPLES_COMPRESSED)
             fail(BSAR_ERR_INVALID_ARG, "unknown samples kind");

@@ -220,6 +220,50 @@ __global__ void k_pulse_compress(const double2* __restrict__ in, int ns, int P, 
     }
 }
 
+// Upsampling of already-compressed pulses into the mixed forms' storage (complex64, or
+// FP16 complex with a per-pulse scale): one CTA per pulse, Hermite weights as above.
+__global__ void k_upsample_store(const double2* __restrict__ in, int64_t n, int factor, int out_kind,
+                                 float2* __restrict__ out32, __half2* __restrict__ out16, float* __restrict__ scale16)
+{
+    __shared__ float red[32];
+    const int64_t p = blockIdx.x;
+    const double2* src = in + p * n;
+    const int64_t nout = n * factor;
+    float scale = 1.0f;
+    if (out_kind == 2) {
+        float m = 0.0f;
+        for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+            double2 v = __ldg(src + i);
+            m = fmaxf(m, fmaxf(fabsf((float)v.x), fabsf((float)v.y)));
+        }
+        for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            m = (threadIdx.x < (blockDim.x >> 5)) ? red[threadIdx.x] : 0.0f;
+            for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+            if (threadIdx.x == 0) red[0] = m;
+        }
+        __syncthreads();
+        m = red[0];
+        scale = (m > 0.0f) ? m / 16384.0f : 1.0f;
+        if (threadIdx.x == 0) scale16[p] = scale;
+    }
+    const float inv_scale = 1.0f / scale;
+    for (int64_t o = threadIdx.x; o < nout; o += blockDim.x) {
+        Hermite H = hermite_at(o, n, factor);
+        int64_t i = H.idx;
+        double2 pm1 = __ldg(src + (i > 0 ? i - 1 : 0)), p0 = __ldg(src + i), p1 = __ldg(src + i + 1);
+        double2 p2 = __ldg(src + (i + 2 < n ? i + 2 : n - 1));
+        double re = hermite_comp(H, n, pm1.x, p0.x, p1.x, p2.x);
+        double im = hermite_comp(H, n, pm1.y, p0.y, p1.y, p2.y);
+        if (out_kind == 1)
+            out32[p * nout + o] = make_float2((float)re, (float)im);
+        else
+            out16[p * nout + o] = __floats2half2_rn((float)re * inv_scale, (float)im * inv_scale);
+    }
+}
+
 // Plain batched FFT rows (natural order in and out) -- FFTProcessor::fft / ::ifft.
 __global__ void k_fft_rows(double2* __restrict__ data, int P, int logP, const double2* __restrict__ tw,
                            int inverse)
@@ -310,6 +354,13 @@ cudaError_t launch_fft_rows(double2* data, int64_t batch, int P, int logP, const
     size_t sm = (size_t)P * sizeof(double2);
     cudaFuncSetAttribute(k_fft_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     k_fft_rows<<<(unsigned)batch, fft_threads(P), sm, st>>>(data, P, logP, tw, inverse);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_upsample_store(const double2* in, int64_t n, int64_t batch, int factor, int out_kind, float2* out32,
+                                  __half2* out16, float* scale16, cudaStream_t st)
+{
+    k_upsample_store<<<(unsigned)batch, 256, 0, st>>>(in, n, factor, out_kind, out32, out16, scale16);
     return cudaGetLastError();
 }
 

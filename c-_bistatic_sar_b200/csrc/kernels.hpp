@@ -36,6 +36,8 @@ cudaError_t launch_fft_rows(double2* data, int64_t batch, int P, int logP, const
                             cudaStream_t st);
 cudaError_t launch_spline(const double2* in, int64_t n, int64_t batch, int factor, double2* out,
                           cudaStream_t st);
+cudaError_t launch_upsample_store(const double2* in, int64_t n, int64_t batch, int factor, int out_kind, float2* out32,
+                                  __half2* out16, float* scale16, cudaStream_t st);
 
 // ------------------------------- Fermat (FP64) ---------------------------------------
 cudaError_t launch_dem_elevation(const DemView& d, const double* xy, int64_t n, double* z, cudaStream_t st);

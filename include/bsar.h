@@ -158,7 +158,8 @@ typedef struct bsar_scene_desc {
     int64_t n_pulses;          /* Np */
     const double* tx;          /* Np x 3 transmitter positions (Tx_positions.csv) */
     const double* rx;          /* Np x 3 receiver positions    (Rx_positions.csv) */
-    int64_t n_samples;         /* Ns fast-time samples per pulse (a power of two)   */
+    int64_t n_samples;         /* Ns fast-time samples per pulse (a power of two for
+                                  raw pulses)                                       */
     const double* samples;     /* Np x Ns complex, pulse-major                       */
     int32_t samples_kind;      /* bsar_samples_kind                                 */
     int32_t upsample;          /* fast-time factor (the reference uses 4,

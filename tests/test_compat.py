@@ -1,0 +1,118 @@
+"""The C++ drop-in layer (libbsar_compat.so, include/bsar_compat.h).
+
+CPU: a driver written against the reference's own headers links against the library
+(same type layouts, same mangled names), and the struct layouts of include/bsar_compat.h
+equal the reference's.
+GPU: the driver runs and its results equal the oracle's (bit-exact Fermat, DEM and spline;
+FFTs to 1e-12), including the reference's non-power-of-two FFT behaviour.
+"""
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import bsar
+import oracle as O
+
+ROOT = Path(__file__).resolve().parent.parent
+LIB = ROOT / "c-_bistatic_sar_b200" / "lib"
+DRIVER = ROOT / "tests" / "compat" / "compat_driver.cpp"
+REF_INC = Path(os.environ.get("BSAR_REFERENCE_TREE", "/root/reference")) / "include"
+
+
+def _build(out: Path, use_bsar_header: bool):
+    if not (LIB / "libbsar_compat.so").exists():
+        bsar.native.build()
+    inc = ["-DUSE_BSAR_HEADER", f"-I{ROOT / 'include'}"] if use_bsar_header else [f"-I{REF_INC}"]
+    cmd = ["/usr/bin/g++", "-O1", "-std=c++17", *inc, str(DRIVER), f"-L{LIB}", "-lbsar_compat",
+           f"-Wl,-rpath,{LIB}", "-o", str(out)]
+    subprocess.run(cmd, check=True, capture_output=True, text=True)
+    return out
+
+
+@pytest.mark.skipif(not REF_INC.exists(), reason="reference headers not present")
+def test_links_against_reference_headers(tmp_path):
+    _build(tmp_path / "drv_ref", use_bsar_header=False)
+
+
+LAYOUT = r'''
+#include <cstddef>
+#include <cstdio>
+#include HEADER
+#define O(T, m) std::printf(#T "." #m " %zu\n", offsetof(T, m))
+int main() {
+  std::printf("RadarTx %zu RadarRx %zu Target %zu System %zu Environment %zu\n", sizeof(RadarTx), sizeof(RadarRx),
+              sizeof(Target), sizeof(System), sizeof(Environment));
+  std::printf("ProcessedDEM %zu TrajectoryMatrix %zu RangeData %zu RawDataResult %zu TrajectoryPoints %zu\n",
+              sizeof(ProcessedDEM), sizeof(TrajectoryMatrix), sizeof(RangeData), sizeof(RawDataResult),
+              sizeof(TrajectoryPoints));
+  O(RadarTx, lamb); O(RadarTx, fs); O(RadarTx, FreqMenor); O(RadarTx, DuracaoPulso); O(RadarRx, fs); O(RadarRx, B);
+  O(System, IndiceMaximo); O(System, PlotarGrafico); O(System, RefGeografico); O(System, ratioUp);
+  O(Target, rcs); O(ProcessedDEM, Z_DEM); O(TrajectoryMatrix, P); O(RawDataResult, chirp);
+  return 0;
+}
+'''
+
+
+@pytest.mark.skipif(not REF_INC.exists(), reason="reference headers not present")
+def test_struct_layouts_match_reference(tmp_path):
+    src = tmp_path / "layout.cpp"
+    src.write_text(LAYOUT)
+    outs = []
+    for hdr, inc in (('"bsar_compat.h"', ROOT / "include"), ('"raw_data_processing.h"', REF_INC)):
+        exe = tmp_path / ("lay" + str(len(outs)))
+        subprocess.run(["/usr/bin/g++", "-std=c++17", f"-DHEADER={hdr}", f"-I{inc}", str(src), "-o", str(exe)],
+                       check=True, capture_output=True, text=True)
+        outs.append(subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout)
+    assert outs[0] == outs[1]
+
+
+def _parse(text):
+    rows = {}
+    for line in text.splitlines():
+        parts = line.split()
+        rows.setdefault(parts[0], []).append([float(v) for v in parts[1:]])
+    return {k: np.array(v) for k, v in rows.items()}
+
+
+@pytest.mark.gpu
+def test_driver_matches_oracle(tmp_path, oracle):
+    exe = _build(tmp_path / "drv", use_bsar_header=True)
+    run = subprocess.run([str(exe)], check=True, capture_output=True, text=True)
+    got = _parse(run.stdout)
+    assert "not a power of 2" in run.stderr
+    xv = 17.0 + 0.5 * np.arange(12)
+    yv = -2.25 + 0.5 * np.arange(10)
+    i, j = np.meshgrid(np.arange(12), np.arange(10))
+    z = 0.02 * i - 0.01 * j + 0.03 * ((i * 7 + j * 3) % 5 - 2)
+    dem = O.Dem(xv, yv, z)
+    k = np.arange(6)
+    tx = np.stack([-4.0 + 1.5 * k, 2.0 - 0.7 * k, np.full(6, 30.0)], 1)
+    rx = tx + [5.0, 0.0, 0.0]
+    P = [20.1, -0.2, -5.0]
+    ranges, ida, _, _ = oracle.slant_range_fermat(dem, tx, rx, P, 1.0, 2.0)
+    assert np.array_equal(got["range"][:, 1:], ranges.T)
+    assert np.array_equal(got["ida"][:, 1:], ida)
+    assert got["elev"][0, 0] == oracle.dem_elevation(dem, [[19.3, 0.4]])[0]
+    assert np.array_equal(got["refr"][0], oracle.refraction_points(dem, tx[:1], [P], 1.0, 2.0)[0])
+    n = np.arange(64)
+    sig = np.cos(0.3 * n) + 1j * np.sin(0.11 * n * n)
+    up = oracle.spline_upsample(sig, 4)[0]
+    idx = got["spline"][:, 0].astype(int)
+    assert np.array_equal(got["spline"][:, 1] + 1j * got["spline"][:, 2], up[idx])
+    corr = oracle.fft_correlate(sig, sig[:16])[0]
+    idx = got["corr"][:, 0].astype(int)
+    c = got["corr"][:, 1] + 1j * got["corr"][:, 2]
+    assert np.abs(c - corr[idx]).max() <= 1e-12 * np.abs(corr).max()
+    f = oracle.fft(sig)
+    assert abs(got["fft0"][0, 0] + 1j * got["fft0"][0, 1] - f[5]) <= 1e-12 * np.abs(f).max()
+    assert got["fftodd"][0, 0] == 1.0
+    nn = np.arange(6 * 256)
+    rc = (np.sin(0.05 * nn) + 1j * np.cos(0.031 * nn)).reshape(6, 256)
+    img = oracle.backproject(dem, tx, rx, rc, [20.0, 20.1], [-0.1, 0.0, 0.1], [-5.0], 1.0, 2.0, 3e8, 2.0e9, 0.3,
+                             legs="mean")
+    gi = got["img"]
+    want = img[gi[:, 0].astype(int), gi[:, 1].astype(int), 0]
+    assert np.abs(gi[:, 2] + 1j * gi[:, 3] - want).max() <= 1e-9 * np.abs(want).max()
