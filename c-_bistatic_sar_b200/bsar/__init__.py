@@ -4,6 +4,7 @@
 ``bsar.scene``   seeded synthetic scenes of the benchmark configurations
 """
 from . import native, scene  # noqa: F401
-from .native import BsarError, Context, DemArrays, upload_scene  # noqa: F401
+from .native import BsarError, Context, DemArrays, Server, submit_scene, synthesize_scene, upload_scene  # noqa: F401
 
-__all__ = ["native", "scene", "Context", "DemArrays", "BsarError", "upload_scene"]
+__all__ = ["native", "scene", "Context", "DemArrays", "BsarError", "Server", "submit_scene", "upload_scene",
+           "synthesize_scene"]

@@ -64,6 +64,24 @@ class Opts(C.Structure):
     _fields_ = [("device", _i32), ("flags", _i32), ("hbm_budget_bytes", C.c_uint64)]
 
 
+class ServerOpts(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_uint64), ("max_inflight", _i32), ("tiles_per_launch", _i32),
+                ("use_graph", _i32), ("reserved", _i32)]
+
+
+class Request(C.Structure):
+    _fields_ = [("scene", SceneDesc), ("scat_pos", _d), ("scat_amp", _d), ("n_scat", _i64),
+                ("snr_db", C.c_double), ("seed", C.c_uint64), ("grid", Grid), ("opts", BpOpts),
+                ("image_out", _d)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
+                ("launches", C.c_uint64), ("tiles", C.c_uint64), ("p50_ms", C.c_double), ("p99_ms", C.c_double),
+                ("mean_ms", C.c_double), ("max_ms", C.c_double), ("voxel_pulses", C.c_double),
+                ("busy_s", C.c_double), ("peak_inflight", C.c_uint64), ("peak_reserved_bytes", C.c_uint64)]
+
+
 def build(quiet: bool = True) -> Path:
     """Compile libbsar.so for sm_100a (nvcc cross-compiles; no GPU needed)."""
     out = subprocess.run(["make", "-C", str(CSRC), "-j4"], capture_output=quiet, text=True)
@@ -103,10 +121,21 @@ def lib() -> C.CDLL:
         "bsar_fft_correlate": ([V, _d, _i64, _i64, _d, _i64, _i32, _d], _i32),
         "bsar_scene_upload": ([V, C.POINTER(SceneDesc), C.POINTER(C.c_uint64)], _i32),
         "bsar_scene_release": ([V, C.c_uint64], _i32),
+        "bsar_scene_synthesize": ([V, C.POINTER(SceneDesc), _d, _d, _i64, C.c_double, C.c_uint64,
+                                   C.POINTER(C.c_uint64)], _i32),
+        "bsar_scene_read_samples": ([V, C.c_uint64, _d], _i32),
         "bsar_scene_compress": ([V, C.c_uint64, _i32], _i32),
         "bsar_scene_read_upsampled": ([V, C.c_uint64, _d], _i32),
+        "bsar_scene_read_stored": ([V, C.c_uint64, _i32, _d], _i32),
         "bsar_backproject": ([V, C.c_uint64, C.POINTER(Grid), C.POINTER(BpOpts), _d], _i32),
         "bsar_backproject_device": ([V, C.c_uint64, C.POINTER(Grid), C.POINTER(BpOpts), V], _i32),
+        "bsar_server_create": ([V, C.POINTER(ServerOpts), C.POINTER(V)], _i32),
+        "bsar_server_submit": ([V, C.POINTER(Request), C.POINTER(C.c_uint64)], _i32),
+        "bsar_server_estimate": ([C.POINTER(Request), C.POINTER(C.c_uint64)], _i32),
+        "bsar_server_poll": ([V, C.c_uint64, C.POINTER(_i32), _d], _i32),
+        "bsar_server_wait": ([V, C.c_uint64, C.c_double, _d], _i32),
+        "bsar_server_get_stats": ([V, C.POINTER(ServerStats)], _i32),
+        "bsar_server_destroy": ([V], None),
     }
     for name, (args, res) in sigs.items():
         fn = getattr(L, name)
@@ -258,6 +287,26 @@ class Context:
         self._ok(self.L.bsar_scene_upload(self.h, C.byref(desc), C.byref(sid)))
         return int(sid.value)
 
+    def scene_synthesize(self, dem: DemArrays, tx, rx, n_samples, scat_pos, scat_amp, *, snr_db=float("inf"),
+                         seed=0, upsample=4, n1=1.0, n2=2.0, c=3e8, fc=1e9, fs=1.2e9, chirp_f0=0.0, chirp_f1=0.0,
+                         chirp_T=0.0) -> int:
+        """Resident raw scene with echoes synthesised on the device (bsar_scene_synthesize)."""
+        tx = _f64(tx, (-1, 3))
+        rx = _f64(rx, (-1, 3))
+        pos = _f64(scat_pos, (-1, 3))
+        amp = _f64(scat_amp)
+        desc = SceneDesc(dem.c, len(tx), _p(tx), _p(rx), int(n_samples), None, 0, upsample, n1, n2, c, fc, fs,
+                         chirp_f0, chirp_f1, chirp_T)
+        sid = C.c_uint64()
+        self._ok(self.L.bsar_scene_synthesize(self.h, C.byref(desc), _p(pos), _p(amp), len(amp), snr_db,
+                                              seed & (2**64 - 1), C.byref(sid)))
+        return int(sid.value)
+
+    def scene_read_samples(self, sid: int, n_pulses: int, n_samples: int):
+        out = np.empty((n_pulses, n_samples), dtype=np.complex128)
+        self._ok(self.L.bsar_scene_read_samples(self.h, sid, _p(out.view(np.float64))))
+        return out
+
     def scene_release(self, sid: int):
         self._ok(self.L.bsar_scene_release(self.h, sid))
 
@@ -267,6 +316,12 @@ class Context:
     def scene_read_upsampled(self, sid: int, n_pulses: int, n_out: int):
         out = np.empty((n_pulses, n_out), dtype=np.complex128)
         self._ok(self.L.bsar_scene_read_upsampled(self.h, sid, _p(out.view(np.float64))))
+        return out
+
+    def scene_read_stored(self, sid: int, n_pulses: int, n_out: int, precision="fp64"):
+        """Upsampled pulses as stored for `precision`, widened to complex128."""
+        out = np.empty((n_pulses, n_out), dtype=np.complex128)
+        self._ok(self.L.bsar_scene_read_stored(self.h, sid, PRECISION[precision], _p(out.view(np.float64))))
         return out
 
     @staticmethod
@@ -289,6 +344,18 @@ class Context:
         self._ok(self.L.bsar_backproject_device(self.h, sid, C.byref(g), C.byref(o), C.c_void_p(d_image_ptr)))
 
 
+def synthesize_scene(ctx: Context, scene, snr_db=None, seed=None) -> int:
+    """Resident raw scene for a bsar.scene.Scene whose echoes are synthesised on the GPU
+    (the scene's DEM, trajectories and scatterers; its numpy `raw` is not used)."""
+    sp = scene.spec
+    dem = DemArrays(scene.x_vec, scene.y_vec, scene.z)
+    f0, f1 = -sp.bandwidth / 2.0, sp.bandwidth / 2.0
+    return ctx.scene_synthesize(dem, scene.tx, scene.rx, sp.n_samples, scene.scat_pos, scene.scat_amp,
+                                snr_db=sp.snr_db if snr_db is None else snr_db,
+                                seed=sp.seed if seed is None else seed, upsample=sp.upsample, n1=sp.n1, n2=sp.n2,
+                                c=3e8, fc=sp.fc, fs=sp.fs, chirp_f0=f0, chirp_f1=f1, chirp_T=sp.pulse_T)
+
+
 def upload_scene(ctx: Context, scene, kind="raw") -> int:
     """Upload a bsar.scene.Scene (raw echoes) to the context."""
     sp = scene.spec
@@ -297,3 +364,130 @@ def upload_scene(ctx: Context, scene, kind="raw") -> int:
     return ctx.scene_upload(dem, scene.tx, scene.rx, scene.raw, kind=kind, upsample=sp.upsample,
                             n1=sp.n1, n2=sp.n2, c=3e8, fc=sp.fc, fs=sp.fs, chirp_f0=f0, chirp_f1=f1,
                             chirp_T=sp.pulse_T)
+
+
+def _request(dem: DemArrays, tx, rx, gx, gy, gz, *, samples=None, n_samples=None, kind="raw", scat_pos=None,
+             scat_amp=None, snr_db=float("inf"), seed=0, upsample=4, n1=1.0, n2=2.0, c=3e8, fc=1e9, fs=1.2e9,
+             chirp_f0=0.0, chirp_f1=0.0, chirp_T=0.0, precision="mixed", search_radius_m=0.0):
+    """bsar_request for the server, the output image and the arrays the request points into."""
+    tx = _f64(tx, (-1, 3))
+    rx = _f64(rx, (-1, 3))
+    keep = [dem, tx, rx]
+    if samples is not None:
+        smp = _c128(samples)
+        keep.append(smp)
+        ns, sp = smp.shape[1], _p(smp.view(np.float64))
+        pos = amp = None
+        nscat = 0
+    else:
+        ns, sp = int(n_samples), None
+        pos = _f64(scat_pos, (-1, 3))
+        amp = _f64(scat_amp)
+        keep += [pos, amp]
+        nscat = len(amp)
+    desc = SceneDesc(dem.c, len(tx), _p(tx), _p(rx), ns, sp, 0 if kind == "raw" else 1, upsample, n1, n2, c, fc, fs,
+                     chirp_f0, chirp_f1, chirp_T)
+    axes, g = Context._grid(gx, gy, gz)
+    keep.append(axes)
+    out = np.empty((g.nx, g.ny, g.nz), dtype=np.complex128)
+    o = BpOpts(SOLVER["newton"], LEGS["per_pulse"], PRECISION[precision], 0, search_radius_m)
+    req = Request(desc, _p(pos), _p(amp), nscat, snr_db, seed & (2**64 - 1), g, o, _p(out.view(np.float64)))
+    return req, out, keep
+
+
+class Server:
+    """Continuous-batching image-formation server on a context (bsar_server_*).
+
+    ``submit`` copies the small arrays; the raw samples (if any) and the output image
+    are kept alive here until the request completes."""
+
+    def __init__(self, ctx: Context, *, hbm_budget_bytes=0, max_inflight=64, tiles_per_launch=0, use_graph=True):
+        self.ctx = ctx
+        self.L = ctx.L
+        h = C.c_void_p()
+        st = self.L.bsar_server_create(ctx.h, C.byref(ServerOpts(hbm_budget_bytes, max_inflight, tiles_per_launch,
+                                                                  1 if use_graph else 0, 0)), C.byref(h))
+        if st != 0:
+            raise BsarError(st, ctx.last_error())
+        self.h = h
+        self._live = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.bsar_server_destroy(self.h)
+            self.h = None
+            self._live.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, dem: DemArrays, tx, rx, gx, gy, gz, **kw) -> int:
+        """Queue one image; echoes come from `samples` or are synthesised on the device
+        from `scat_pos`/`scat_amp` (then `n_samples` gives the pulse length).  Keyword
+        arguments as in :func:`_request`."""
+        req, out, keep = _request(dem, tx, rx, gx, gy, gz, **kw)
+        rid = C.c_uint64()
+        st = self.L.bsar_server_submit(self.h, C.byref(req), C.byref(rid))
+        if st != 0:
+            raise BsarError(st, "request rejected")
+        self._live[int(rid.value)] = (out, keep)
+        return int(rid.value)
+
+    @staticmethod
+    def estimate(dem: DemArrays, tx, rx, gx, gy, gz, **kw) -> int:
+        """Device bytes the request would reserve against a server's budget."""
+        req, _, _ = _request(dem, tx, rx, gx, gy, gz, **kw)
+        b = C.c_uint64()
+        st = lib().bsar_server_estimate(C.byref(req), C.byref(b))
+        if st != 0:
+            raise BsarError(st, "estimate")
+        return int(b.value)
+
+    def poll(self, rid: int):
+        """(done, latency_ms); raises when the request failed."""
+        done = _i32()
+        lat = C.c_double()
+        st = self.L.bsar_server_poll(self.h, rid, C.byref(done), C.byref(lat))
+        if st != 0:
+            raise BsarError(st, f"request {rid} failed")
+        return bool(done.value), float(lat.value)
+
+    def wait(self, rid: int, timeout_s: float = 600.0):
+        """Image and latency (ms) of a request; raises when it failed or timed out."""
+        lat = C.c_double()
+        st = self.L.bsar_server_wait(self.h, rid, timeout_s, C.byref(lat))
+        if st != 0:
+            raise BsarError(st, f"request {rid}")
+        out, _ = self._live.pop(rid)
+        return out, float(lat.value)
+
+    def stats(self) -> dict:
+        o = ServerStats()
+        st = self.L.bsar_server_get_stats(self.h, C.byref(o))
+        if st != 0:
+            raise BsarError(st, "stats")
+        return {k: getattr(o, k) for k, _ in ServerStats._fields_}
+
+
+def submit_scene(server: Server, scene, gx, gy, gz, *, synthesize=True, precision="mixed", snr_db=None, seed=None):
+    """Queue a bsar.scene.Scene on a server: echoes synthesised on the device from the
+    scene's scatterers (default) or uploaded from its numpy `raw`."""
+    sp = scene.spec
+    dem = DemArrays(scene.x_vec, scene.y_vec, scene.z)
+    f0, f1 = -sp.bandwidth / 2.0, sp.bandwidth / 2.0
+    common = dict(upsample=sp.upsample, n1=sp.n1, n2=sp.n2, c=3e8, fc=sp.fc, fs=sp.fs, chirp_f0=f0, chirp_f1=f1,
+                  chirp_T=sp.pulse_T, precision=precision)
+    if synthesize:
+        return server.submit(dem, scene.tx, scene.rx, gx, gy, gz, n_samples=sp.n_samples, scat_pos=scene.scat_pos,
+                             scat_amp=scene.scat_amp, snr_db=sp.snr_db if snr_db is None else snr_db,
+                             seed=sp.seed if seed is None else seed, **common)
+    return server.submit(dem, scene.tx, scene.rx, gx, gy, gz, samples=scene.raw, **common)

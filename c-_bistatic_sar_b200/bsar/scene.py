@@ -440,3 +440,64 @@ def make_scene(spec: SceneSpec, with_raw: bool = True) -> Scene:
 def pulse_compress_np(raw: np.ndarray, reference: np.ndarray) -> np.ndarray:
     """numpy pulse compression ifft(fft(raw) * conj(fft(ref))) per pulse (a cross-check)."""
     return np.fft.ifft(np.fft.fft(raw, axis=1) * np.conj(np.fft.fft(reference))[None, :], axis=1)
+
+
+# ------------------------------------------------------------------------------------
+# Served mixed workload: image-formation requests of different sizes over a few
+# resident DEMs, arriving as a Poisson stream.
+@dataclass
+class ServeMix:
+    dems: list                  # [(x_vec, y_vec, z, eps_r, sigma)]
+    requests: list              # [Scene] (raw echoes not generated: synthesised on the device)
+    dem_index: np.ndarray       # DEM of each request
+
+
+def serve_mix(n_requests: int = 512, seed: int = SEED_BASE + 4, n_dems: int = 8, side=(21, 161),
+              pulses=(128, 2048), samples_log2=(11, 14), scatterers=(5, 50), sigma=(0.1, 0.5),
+              eps_r=(3.0, 9.0)) -> ServeMix:
+    """Seeded request list of the served workload.
+
+    Per request: grid side log-uniform over `side` (x = y = side, z = ceil(side / 2), 0.02 m
+    voxels centred 20 m downrange and 5 m deep), pulse count log-uniform over `pulses`,
+    fast-time samples 2^k with k uniform over `samples_log2` (log-uniform over powers of
+    two), scatterer count uniform over `scatterers`, one of `n_dems` fBm DEMs (256 x 256
+    at 0.25 m, beta 2, sigma uniform over `sigma`, eps_r uniform over `eps_r`).  Signal as
+    the medium scene: f_c 1 GHz, B 800 MHz, fs 1.92 GHz, 1 us chirp, 15 dB SNR."""
+    s_dem, s_req = np.random.SeedSequence(seed).spawn(2)
+    rng_d = np.random.Generator(np.random.PCG64(s_dem))
+    rng = np.random.Generator(np.random.PCG64(s_req))
+    base = config_spec(2)
+    dems = []
+    for k in range(n_dems):
+        sg = float(rng_d.uniform(*sigma))
+        er = float(rng_d.uniform(*eps_r))
+        dspec = replace(base, name=f"serve-dem{k}", dem_sigma=sg, eps_r=er)
+        x_vec, y_vec, z = make_dem(dspec, rng_d)
+        dems.append((x_vec, y_vec, z, er, sg))
+    reqs, dem_idx = [], []
+    for i in range(n_requests):
+        sd = int(round(math.exp(rng.uniform(math.log(side[0]), math.log(side[1])))))
+        npl = int(round(math.exp(rng.uniform(math.log(pulses[0]), math.log(pulses[1])))))
+        ns = 1 << int(rng.integers(samples_log2[0], samples_log2[1] + 1))
+        nsc = int(rng.integers(scatterers[0], scatterers[1] + 1))
+        k = int(rng.integers(0, n_dems))
+        rseed = int(rng.integers(0, 2**62))
+        x_vec, y_vec, z, er, sg = dems[k]
+        spec = replace(base, name=f"serve-req{i}", nx=sd, ny=sd, nz=(sd + 1) // 2, dem_sigma=sg, eps_r=er,
+                       n_pulses=npl, n_samples=ns, n_scatterers=nsc, seed=rseed)
+        _, rng_scat, _, _ = _streams(rseed)
+        tx, rx = make_trajectories(spec)
+        gx, gy, gz = grid_axes(spec)
+        pos, amp, vox = make_scatterers(spec, rng_scat, gx, gy, gz)
+        sc = Scene(spec, x_vec, y_vec, z, tx, rx, gx, gy, gz, pos, amp, vox)
+        reqs.append(sc)
+        dem_idx.append(k)
+    return ServeMix(dems, reqs, np.asarray(dem_idx))
+
+
+def poisson_arrivals(n: int, rate_per_s: float, seed: int = SEED_BASE + 40) -> np.ndarray:
+    """Arrival times (s) of a Poisson stream: cumulative exponential gaps, first at 0."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    gaps = rng.exponential(1.0 / rate_per_s, size=n)
+    gaps[0] = 0.0
+    return np.cumsum(gaps)

@@ -1,0 +1,661 @@
+// bsar_serve.cpp -- continuous-batching image-formation server (bsar_server_* of bsar.h).
+//
+// One worker thread per server owns the GPU work:
+//
+//   loop:
+//     launch the next batch (async, `run` stream): the persistent mixed kernel over a
+//       fair-share list of (request, 128-voxel tile) work items of every active request,
+//       as a replay of a captured CUDA graph (copy of the request records and the tile
+//       list from pinned staging, zeroed work counter, kernel)
+//     while it runs: admit pending requests FIFO while the HBM budget and the in-flight
+//       slots allow (scene upload or on-device echo synthesis, pulse compression +
+//       upsampling, per-pulse anchors; `io` stream)
+//     wait for the batch (bounded), retire requests whose tiles are all done (image to
+//       the caller's buffer, resources released, latency recorded)
+//
+// Work items are the same 128-voxel groups a one-request launch uses, so every voxel's
+// arithmetic is independent of the batch it runs in.
+#include "runtime.hpp"
+
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <thread>
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+constexpr int kMaxSlots = 256;
+constexpr double kBatchTimeoutS = 300.0;   // bounded wait for one batch
+
+enum class St { Pending, Active, Done, Failed };
+
+struct Req {
+    uint64_t id = 0;
+    St state = St::Pending;
+    bsar_status status = BSAR_OK;
+    std::string error;
+    // copies of the request's small arrays
+    std::vector<double> dem_x, dem_y, dem_z, tx, rx, gx, gy, gz, spos, samp;
+    bsar_scene_desc desc{};
+    bsar_grid grid{};
+    bsar_bp_opts opts{};
+    int64_t n_scat = 0;
+    double snr_db = 0;
+    uint64_t seed = 0;
+    double* image_out = nullptr;
+    // device state while admitted
+    int slot = -1;
+    uint64_t reserved = 0;
+    std::unique_ptr<Scene> scene;
+    std::unique_ptr<DevBuf> axes, image;
+    MixedReq rec{};
+    int64_t ntiles = 0, next_tile = 0, done_tiles = 0;
+    Clock::time_point t_submit, t_done;
+    double voxel_pulses = 0;
+};
+
+uint64_t estimate_bytes(const Req& r)
+{
+    const uint64_t np = r.desc.n_pulses, ns = r.desc.n_samples, up = r.desc.upsample;
+    const uint64_t nd = (uint64_t)std::max<int64_t>(r.desc.dem.nx, 1) * std::max<int64_t>(r.desc.dem.ny, 1);
+    const uint64_t nv = (uint64_t)r.grid.nx * r.grid.ny * r.grid.nz;
+    const uint64_t sample = r.opts.precision == BSAR_MIXED_FP16 ? 4 : 8;
+    return 16 * np * ns                              // raw pulses
+           + sample * np * ns * up                   // upsampled pulses
+           + 16 * ns + 16 * nv                       // spectrum, image
+           + 12 * nd + 48 * np + 52 * np             // DEM, trajectories, anchors
+           + 24 * np * (uint64_t)std::max<int64_t>(r.n_scat, 1)   // synthesis work buffers
+           + (1u << 20);
+}
+
+}  // namespace
+
+struct bsar_server {
+    bsar_ctx* ctx = nullptr;
+    bsar_server_opts opts{};
+    uint64_t budget = 0, reserved = 0;
+    std::thread worker;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    bool stop = false;
+    uint64_t next_id = 1;
+    std::deque<Req*> pending;
+    std::vector<Req*> active;                       // admission order
+    std::map<uint64_t, std::unique_ptr<Req>> reqs;
+    bool slot_used[kMaxSlots] = {};
+    // batch staging (pinned) and device copies
+    MixedReq* h_reqs = nullptr;
+    int2* h_tiles = nullptr;
+    int* h_ntiles = nullptr;
+    std::unique_ptr<DevBuf> d_reqs, d_tiles, d_ntiles, d_counter;
+    cudaStream_t run = nullptr, io = nullptr;
+    cudaEvent_t ev_done = nullptr;
+    std::map<int, cudaGraphExec_t> graphs;         // per node-scan width W
+    int grid_ctas = 0, max_tiles = 0;
+    // statistics
+    std::vector<double> latencies;
+    uint64_t submitted = 0, completed = 0, failed = 0, launches = 0, tiles = 0;
+    uint64_t peak_inflight = 0, peak_reserved = 0;
+    double vp_done = 0;
+    bool any_submit = false;
+    Clock::time_point t_first, t_last;
+    std::string fatal;
+};
+
+namespace {
+
+// Runs `f` with the context locked and its stream switched to `st`.
+template <typename F> void with_ctx(bsar_server* s, cudaStream_t st, F&& f)
+{
+    std::lock_guard<std::mutex> lk(s->ctx->mu);
+    cudaStream_t saved = s->ctx->stream;
+    s->ctx->stream = st;
+    try {
+        f();
+    } catch (...) {
+        s->ctx->stream = saved;
+        throw;
+    }
+    s->ctx->stream = saved;
+}
+
+void finish(bsar_server* s, Req* r, bsar_status st, const std::string& err)
+{
+    r->status = st;
+    r->error = err;
+    r->state = st == BSAR_OK ? St::Done : St::Failed;
+    r->t_done = Clock::now();
+    if (r->slot >= 0) s->slot_used[r->slot] = false;
+    r->slot = -1;
+    s->reserved -= r->reserved;
+    r->reserved = 0;
+    if (st == BSAR_OK) {
+        s->completed++;
+        s->vp_done += r->voxel_pulses;
+        s->latencies.push_back(std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count());
+        s->t_last = r->t_done;
+    } else {
+        s->failed++;
+    }
+}
+
+void release(bsar_server* s, Req* r)
+{
+    with_ctx(s, s->io, [&] {
+        r->scene.reset();
+        r->axes.reset();
+        r->image.reset();
+    });
+}
+
+// Admission of one request (worker thread, server lock NOT held): scene upload or
+// synthesis, pulse compression + upsampling, anchors, device image.
+void admit(bsar_server* s, Req* r)
+{
+    with_ctx(s, s->io, [&] {
+        bsar_ctx* ctx = s->ctx;
+        bsar_scene_desc d = r->desc;
+        const bool synth = d.samples == nullptr;
+        r->scene = make_scene(ctx, d, !synth);
+        if (synth) synthesize_samples(ctx, r->scene.get(), r->spos.data(), r->samp.data(), r->n_scat, r->snr_db, r->seed);
+        check_newton_dem(r->scene->dem.view);
+        if (r->scene->dem.view.empty || r->scene->dem.view.nx < 2 || r->scene->dem.view.ny < 2)
+            fail(BSAR_ERR_UNSUPPORTED, "the mixed forms need a DEM of at least 2 x 2 nodes");
+        compress_scene(ctx, r->scene.get(), r->opts.precision);
+        sync(ctx);
+        r->scene->samples.reset();        // only the upsampled pulses are needed from here
+        std::vector<double> ax;
+        ax.insert(ax.end(), r->gx.begin(), r->gx.end());
+        ax.insert(ax.end(), r->gy.begin(), r->gy.end());
+        ax.insert(ax.end(), r->gz.begin(), r->gz.end());
+        r->axes = dev_upload(ctx, ax.data(), sizeof(double) * ax.size());
+        const int64_t nv = r->grid.nx * r->grid.ny * r->grid.nz;
+        r->image = dev_alloc(ctx, sizeof(double2) * nv);
+        Scene* sc = r->scene.get();
+        BpArgs a{};
+        a.dem = sc->dem.view;
+        a.tx = sc->tx->as<double>();
+        a.rx = sc->rx->as<double>();
+        a.np = (int)sc->np;
+        a.nr = sc->nr;
+        a.rc32 = sc->rc[BSAR_MIXED].data ? sc->rc[BSAR_MIXED].data->as<float2>() : nullptr;
+        a.rc16 = sc->rc[BSAR_MIXED_FP16].data ? sc->rc[BSAR_MIXED_FP16].data->as<__half2>() : nullptr;
+        a.scale16 = sc->rc[BSAR_MIXED_FP16].scale ? sc->rc[BSAR_MIXED_FP16].scale->as<float>() : nullptr;
+        a.gx = r->axes->as<double>();
+        a.gy = a.gx + r->grid.nx;
+        a.gz = a.gy + r->grid.ny;
+        a.nx = (int)r->grid.nx;
+        a.ny = (int)r->grid.ny;
+        a.nz = (int)r->grid.nz;
+        a.n1 = sc->n1;
+        a.n2 = sc->n2;
+        a.c = sc->c;
+        a.fs_eff = sc->fs * sc->upsample;
+        a.lambda = sc->c / sc->fc;
+        a.W = search_nodes(sc->dem.view, r->opts.search_radius_m);
+        a.v_begin = 0;
+        a.v_count = nv;
+        a.out = r->image->as<double2>();
+        bsar_grid g = r->grid;
+        g.x_axis = r->gx.data();
+        g.y_axis = r->gy.data();
+        g.z_axis = r->gz.data();
+        set_anchors(ctx, sc, &g, a);
+        sync(ctx);
+        r->rec = mixed_request(sc, a, r->opts.precision == BSAR_MIXED_FP16);
+        r->ntiles = (nv + 127) / 128;
+        r->voxel_pulses = (double)nv * (double)sc->np;
+    });
+}
+
+// Fair-share batch: equal tile chunks to every active request, oldest first.
+int build_batch(bsar_server* s, int* W_out)
+{
+    int n = 0, W = -1;
+    bool mixedW = false;
+    std::vector<Req*> live;
+    for (Req* r : s->active)
+        if (r->next_tile < r->ntiles) live.push_back(r);
+    if (live.empty()) return 0;
+    const int chunk = std::max(1, s->max_tiles / (int)live.size());
+    bool progress = true;
+    while (n < s->max_tiles && progress) {
+        progress = false;
+        for (Req* r : live) {
+            int64_t take = std::min<int64_t>({(int64_t)chunk, r->ntiles - r->next_tile, (int64_t)(s->max_tiles - n)});
+            for (int64_t t = 0; t < take; t++) s->h_tiles[n++] = make_int2(r->slot, (int)(r->next_tile + t));
+            if (take > 0) {
+                r->next_tile += take;
+                progress = true;
+                if (W < 0) W = r->rec.a.W;
+                else if (W != r->rec.a.W) mixedW = true;
+            }
+            if (n >= s->max_tiles) break;
+        }
+    }
+    for (Req* r : s->active) s->h_reqs[r->slot] = r->rec;
+    *s->h_ntiles = n;
+    *W_out = mixedW ? 0 : W;
+    return n;
+}
+
+// Captured graph of one batch launch: staging copies, counter reset, persistent kernel.
+cudaGraphExec_t batch_graph(bsar_server* s, int W)
+{
+    auto it = s->graphs.find(W);
+    if (it != s->graphs.end()) return it->second;
+    MixedBatch b{s->d_reqs->as<MixedReq>(), s->d_tiles->as<int2>(), s->d_ntiles->as<int>(), 0,
+                 s->d_counter->as<int>(), s->ctx->status->as<int>()};
+    cudaGraph_t g = nullptr;
+    cuda_check(cudaStreamBeginCapture(s->run, cudaStreamCaptureModeThreadLocal), "begin capture");
+    cudaMemcpyAsync(s->d_reqs->p, s->h_reqs, sizeof(MixedReq) * kMaxSlots, cudaMemcpyHostToDevice, s->run);
+    cudaMemcpyAsync(s->d_tiles->p, s->h_tiles, sizeof(int2) * s->max_tiles, cudaMemcpyHostToDevice, s->run);
+    cudaMemcpyAsync(s->d_ntiles->p, s->h_ntiles, sizeof(int), cudaMemcpyHostToDevice, s->run);
+    cudaMemsetAsync(s->d_counter->p, 0, sizeof(int), s->run);
+    cudaError_t le = launch_bp_mixed(b, W, s->grid_ctas, s->run);
+    cudaError_t ce = cudaStreamEndCapture(s->run, &g);
+    cuda_check(le, "batch launch (capture)");
+    cuda_check(ce, "end capture");
+    cudaGraphExec_t exec = nullptr;
+    cuda_check(cudaGraphInstantiate(&exec, g, 0), "graph instantiate");
+    cudaGraphDestroy(g);
+    s->graphs[W] = exec;
+    return exec;
+}
+
+void launch_batch(bsar_server* s, int W, int n)
+{
+    if (s->opts.use_graph) {
+        cuda_check(cudaGraphLaunch(batch_graph(s, W), s->run), "graph launch");
+    } else {
+        MixedBatch b{s->d_reqs->as<MixedReq>(), s->d_tiles->as<int2>(), nullptr, n, s->d_counter->as<int>(),
+                     s->ctx->status->as<int>()};
+        cuda_check(cudaMemcpyAsync(s->d_reqs->p, s->h_reqs, sizeof(MixedReq) * kMaxSlots, cudaMemcpyHostToDevice, s->run),
+                   "h2d");
+        cuda_check(cudaMemcpyAsync(s->d_tiles->p, s->h_tiles, sizeof(int2) * n, cudaMemcpyHostToDevice, s->run), "h2d");
+        cuda_check(cudaMemsetAsync(s->d_counter->p, 0, sizeof(int), s->run), "memset");
+        cuda_check(launch_bp_mixed(b, W, std::min(n, s->grid_ctas), s->run), "batch launch");
+    }
+    cuda_check(cudaEventRecord(s->ev_done, s->run), "event");
+    s->launches++;
+    s->tiles += n;
+}
+
+bool wait_batch(bsar_server* s)
+{
+    const auto t0 = Clock::now();
+    for (;;) {
+        cudaError_t e = cudaEventQuery(s->ev_done);
+        if (e == cudaSuccess) return true;
+        if (e != cudaErrorNotReady) fail(BSAR_ERR_CUDA, "batch: %s", cudaGetErrorString(e));
+        if (std::chrono::duration<double>(Clock::now() - t0).count() > kBatchTimeoutS) return false;
+        std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
+}
+
+// Admits pending requests while budget and slots allow (server lock held on entry and
+// exit; released around the device work).
+void admit_pending(bsar_server* s, std::unique_lock<std::mutex>& lk)
+{
+    while (!s->pending.empty() && !s->stop) {
+        Req* r = s->pending.front();
+        const uint64_t need = estimate_bytes(*r);
+        int slot = -1;
+        for (int k = 0; k < s->opts.max_inflight; k++)
+            if (!s->slot_used[k]) {
+                slot = k;
+                break;
+            }
+        if (slot < 0) return;
+        if (s->reserved + need > s->budget && !s->active.empty()) return;
+        s->pending.pop_front();
+        s->slot_used[slot] = true;
+        r->slot = slot;
+        r->reserved = need;
+        s->reserved += need;
+        s->peak_reserved = std::max(s->peak_reserved, s->reserved);
+        lk.unlock();
+        bsar_status st = BSAR_OK;
+        std::string err;
+        try {
+            if (need > s->budget) fail(BSAR_ERR_OOM_BUDGET, "request needs %llu bytes, the server budget is %llu",
+                                       (unsigned long long)need, (unsigned long long)s->budget);
+            admit(s, r);
+        } catch (const Error& e) {
+            st = e.status;
+            err = e.msg;
+        } catch (const std::bad_alloc&) {
+            st = BSAR_ERR_OOM_BUDGET;
+            err = "host allocation failed";
+        }
+        if (st != BSAR_OK) release(s, r);
+        lk.lock();
+        if (st == BSAR_OK) {
+            r->state = St::Active;
+            s->active.push_back(r);
+            s->peak_inflight = std::max<uint64_t>(s->peak_inflight, s->active.size());
+        } else {
+            finish(s, r, st, err);
+            s->cv_done.notify_all();
+        }
+    }
+}
+
+void retire_finished(bsar_server* s, std::unique_lock<std::mutex>& lk)
+{
+    std::vector<Req*> done;
+    for (Req* r : s->active)
+        if (r->done_tiles >= r->ntiles) done.push_back(r);
+    for (Req* r : done) {
+        s->active.erase(std::find(s->active.begin(), s->active.end(), r));
+        lk.unlock();
+        bsar_status st = BSAR_OK;
+        std::string err;
+        try {
+            with_ctx(s, s->io, [&] {
+                cuda_check(cudaMemcpyAsync(r->image_out, r->image->p, r->image->bytes, cudaMemcpyDeviceToHost, s->io),
+                           "image d2h");
+                sync(s->ctx);
+            });
+        } catch (const Error& e) {
+            st = e.status;
+            err = e.msg;
+        }
+        release(s, r);
+        lk.lock();
+        finish(s, r, st, err);
+    }
+    if (!done.empty()) s->cv_done.notify_all();
+}
+
+void worker_main(bsar_server* s)
+{
+    cudaSetDevice(s->ctx->device);
+    std::unique_lock<std::mutex> lk(s->mu);
+    while (true) {
+        if (s->stop) break;
+        // 1. next batch
+        int W = 0;
+        const int n = build_batch(s, &W);
+        std::vector<std::pair<Req*, int64_t>> in_batch;
+        if (n > 0) {
+            std::map<int, int64_t> per_slot;
+            for (int k = 0; k < n; k++) per_slot[s->h_tiles[k].x]++;
+            for (Req* r : s->active)
+                if (per_slot.count(r->slot)) in_batch.push_back({r, per_slot[r->slot]});
+            try {
+                with_ctx(s, s->run, [&] { launch_batch(s, W, n); });
+            } catch (const Error& e) {
+                s->fatal = e.msg;
+                break;
+            }
+        }
+        // 2. admit while it runs
+        admit_pending(s, lk);
+        // 3. wait and retire
+        if (n > 0) {
+            lk.unlock();
+            bool ok = false;
+            std::string err;
+            try {
+                ok = wait_batch(s);
+            } catch (const Error& e) {
+                err = e.msg;
+            }
+            lk.lock();
+            if (!ok) {
+                s->fatal = err.empty() ? "a batch did not finish within its time limit" : err;
+                for (auto& p : in_batch) {
+                    s->active.erase(std::find(s->active.begin(), s->active.end(), p.first));
+                    finish(s, p.first, err.empty() ? BSAR_ERR_TIMEOUT : BSAR_ERR_CUDA, s->fatal);
+                }
+                s->cv_done.notify_all();
+                break;
+            }
+            // a bounded device wait that ran out fails this batch's requests
+            std::string serr;
+            try {
+                with_ctx(s, s->run, [&] { check_device_status(s->ctx); });
+            } catch (const Error& e) {
+                serr = e.msg;
+            }
+            for (auto& p : in_batch) {
+                if (!serr.empty()) {
+                    s->active.erase(std::find(s->active.begin(), s->active.end(), p.first));
+                    lk.unlock();
+                    release(s, p.first);
+                    lk.lock();
+                    finish(s, p.first, BSAR_ERR_TIMEOUT, serr);
+                } else {
+                    p.first->done_tiles += p.second;
+                }
+            }
+            if (!serr.empty()) s->cv_done.notify_all();
+            retire_finished(s, lk);
+        } else if (s->pending.empty() || s->active.size() >= (size_t)s->opts.max_inflight) {
+            s->cv_work.wait_for(lk, std::chrono::milliseconds(2));
+        }
+    }
+    // fail whatever is left
+    for (Req* r : s->active) finish(s, r, BSAR_ERR_CUDA, s->fatal.empty() ? "server stopped" : s->fatal);
+    s->active.clear();
+    for (Req* r : s->pending) finish(s, r, BSAR_ERR_CUDA, s->fatal.empty() ? "server stopped" : s->fatal);
+    s->pending.clear();
+    s->cv_done.notify_all();
+}
+
+double percentile(std::vector<double> v, double p)
+{
+    if (v.empty()) return 0.0;
+    std::sort(v.begin(), v.end());
+    double idx = p * (double)(v.size() - 1);
+    size_t lo = (size_t)idx;
+    size_t hi = std::min(lo + 1, v.size() - 1);
+    return v[lo] + (idx - (double)lo) * (v[hi] - v[lo]);
+}
+
+}  // namespace
+
+extern "C" {
+
+bsar_status bsar_server_create(bsar_ctx* ctx, const bsar_server_opts* opts, bsar_server** out)
+{
+    if (!ctx || !out) return BSAR_ERR_INVALID_ARG;
+    *out = nullptr;
+    auto s = std::make_unique<bsar_server>();
+    s->ctx = ctx;
+    if (opts) s->opts = *opts;
+    if (s->opts.max_inflight <= 0) s->opts.max_inflight = 64;
+    if (s->opts.max_inflight > kMaxSlots) return BSAR_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    try {
+        cuda_check(cudaSetDevice(ctx->device), "cudaSetDevice");
+        s->grid_ctas = mixed_grid_ctas();
+        s->max_tiles = s->opts.tiles_per_launch > 0 ? s->opts.tiles_per_launch : 2 * s->grid_ctas;
+        const uint64_t free_budget = ctx->budget > ctx->used ? ctx->budget - ctx->used : 0;
+        s->budget = s->opts.hbm_budget_bytes ? s->opts.hbm_budget_bytes : (uint64_t)(0.9 * (double)free_budget);
+        cuda_check(cudaStreamCreateWithFlags(&s->run, cudaStreamNonBlocking), "stream");
+        cuda_check(cudaStreamCreateWithFlags(&s->io, cudaStreamNonBlocking), "stream");
+        cuda_check(cudaEventCreateWithFlags(&s->ev_done, cudaEventDisableTiming), "event");
+        cuda_check(cudaMallocHost((void**)&s->h_reqs, sizeof(MixedReq) * kMaxSlots), "pinned");
+        cuda_check(cudaMallocHost((void**)&s->h_tiles, sizeof(int2) * s->max_tiles), "pinned");
+        cuda_check(cudaMallocHost((void**)&s->h_ntiles, sizeof(int)), "pinned");
+        std::memset(s->h_reqs, 0, sizeof(MixedReq) * kMaxSlots);
+        s->d_reqs = dev_alloc(ctx, sizeof(MixedReq) * kMaxSlots);
+        s->d_tiles = dev_alloc(ctx, sizeof(int2) * s->max_tiles);
+        s->d_ntiles = dev_alloc(ctx, sizeof(int));
+        s->d_counter = dev_alloc(ctx, sizeof(int));
+        if (!ctx->status) {
+            ctx->status = dev_alloc(ctx, sizeof(int));
+            cuda_check(cudaMemset(ctx->status->p, 0, sizeof(int)), "memset");
+        }
+    } catch (const Error& e) {
+        ctx->last_error = e.msg;
+        return e.status;
+    }
+    bsar_server* raw = s.release();
+    raw->worker = std::thread(worker_main, raw);
+    *out = raw;
+    return BSAR_OK;
+}
+
+bsar_status bsar_server_submit(bsar_server* s, const bsar_request* q, bsar_request_id* out)
+{
+    if (!s || !q || !out) return BSAR_ERR_INVALID_ARG;
+    auto r = std::make_unique<Req>();
+    const bsar_scene_desc& d = q->scene;
+    const int64_t np = d.n_pulses;
+    if (np < 1 || !d.tx || !d.rx || d.dem.nx < 2 || d.dem.ny < 2 || !d.dem.x_vec || !d.dem.y_vec || !d.dem.z)
+        return BSAR_ERR_INVALID_ARG;
+    if (q->grid.nx < 1 || q->grid.ny < 1 || q->grid.nz < 1 || !q->grid.x_axis || !q->grid.y_axis || !q->grid.z_axis ||
+        !q->image_out)
+        return BSAR_ERR_INVALID_ARG;
+    if (q->opts.solver != BSAR_SOLVER_NEWTON || q->opts.legs != BSAR_LEGS_PER_PULSE ||
+        (q->opts.precision != BSAR_MIXED && q->opts.precision != BSAR_MIXED_FP16))
+        return BSAR_ERR_UNSUPPORTED;
+    if (!d.samples && (q->n_scat < 0 || (q->n_scat > 0 && (!q->scat_pos || !q->scat_amp))))
+        return BSAR_ERR_INVALID_ARG;
+    r->dem_x.assign(d.dem.x_vec, d.dem.x_vec + d.dem.nx);
+    r->dem_y.assign(d.dem.y_vec, d.dem.y_vec + d.dem.ny);
+    r->dem_z.assign(d.dem.z, d.dem.z + d.dem.nx * d.dem.ny);
+    r->tx.assign(d.tx, d.tx + 3 * np);
+    r->rx.assign(d.rx, d.rx + 3 * np);
+    r->gx.assign(q->grid.x_axis, q->grid.x_axis + q->grid.nx);
+    r->gy.assign(q->grid.y_axis, q->grid.y_axis + q->grid.ny);
+    r->gz.assign(q->grid.z_axis, q->grid.z_axis + q->grid.nz);
+    if (!d.samples && q->n_scat > 0) {
+        r->spos.assign(q->scat_pos, q->scat_pos + 3 * q->n_scat);
+        r->samp.assign(q->scat_amp, q->scat_amp + q->n_scat);
+    }
+    r->desc = d;
+    r->desc.dem.x_vec = r->dem_x.data();
+    r->desc.dem.y_vec = r->dem_y.data();
+    r->desc.dem.z = r->dem_z.data();
+    r->desc.tx = r->tx.data();
+    r->desc.rx = r->rx.data();
+    r->grid = q->grid;
+    r->opts = q->opts;
+    r->n_scat = d.samples ? 0 : q->n_scat;
+    r->snr_db = q->snr_db;
+    r->seed = q->seed;
+    r->image_out = q->image_out;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->stop || !s->fatal.empty()) return BSAR_ERR_CUDA;
+    r->id = s->next_id++;
+    r->t_submit = Clock::now();
+    if (!s->any_submit) {
+        s->any_submit = true;
+        s->t_first = r->t_submit;
+    }
+    s->submitted++;
+    *out = r->id;
+    s->pending.push_back(r.get());
+    s->reqs[r->id] = std::move(r);
+    s->cv_work.notify_all();
+    return BSAR_OK;
+}
+
+bsar_status bsar_server_estimate(const bsar_request* q, uint64_t* bytes)
+{
+    if (!q || !bytes) return BSAR_ERR_INVALID_ARG;
+    Req r;
+    r.desc = q->scene;
+    r.grid = q->grid;
+    r.opts = q->opts;
+    r.n_scat = q->scene.samples ? 0 : q->n_scat;
+    *bytes = estimate_bytes(r);
+    return BSAR_OK;
+}
+
+bsar_status bsar_server_poll(bsar_server* s, bsar_request_id id, int32_t* done, double* latency_ms)
+{
+    if (!s || !done) return BSAR_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(id);
+    if (it == s->reqs.end()) return BSAR_ERR_NOT_FOUND;
+    Req* r = it->second.get();
+    *done = (r->state == St::Done || r->state == St::Failed) ? 1 : 0;
+    if (!*done) return BSAR_OK;
+    if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count();
+    return r->status;
+}
+
+bsar_status bsar_server_wait(bsar_server* s, bsar_request_id id, double timeout_s, double* latency_ms)
+{
+    if (!s) return BSAR_ERR_INVALID_ARG;
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(id);
+    if (it == s->reqs.end()) return BSAR_ERR_NOT_FOUND;
+    Req* r = it->second.get();
+    const auto deadline = Clock::now() + std::chrono::duration_cast<Clock::duration>(std::chrono::duration<double>(timeout_s));
+    while (r->state != St::Done && r->state != St::Failed) {
+        if (s->cv_done.wait_until(lk, deadline) == std::cv_status::timeout &&
+            r->state != St::Done && r->state != St::Failed)
+            return BSAR_ERR_TIMEOUT;
+    }
+    if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count();
+    return r->status;
+}
+
+bsar_status bsar_server_get_stats(bsar_server* s, bsar_server_stats* o)
+{
+    if (!s || !o) return BSAR_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    o->submitted = s->submitted;
+    o->completed = s->completed;
+    o->failed = s->failed;
+    o->launches = s->launches;
+    o->tiles = s->tiles;
+    o->p50_ms = percentile(s->latencies, 0.50);
+    o->p99_ms = percentile(s->latencies, 0.99);
+    double sum = 0, mx = 0;
+    for (double v : s->latencies) {
+        sum += v;
+        mx = std::max(mx, v);
+    }
+    o->mean_ms = s->latencies.empty() ? 0.0 : sum / s->latencies.size();
+    o->max_ms = mx;
+    o->voxel_pulses = s->vp_done;
+    o->busy_s = s->completed ? std::chrono::duration<double>(s->t_last - s->t_first).count() : 0.0;
+    o->peak_inflight = s->peak_inflight;
+    o->peak_reserved_bytes = s->peak_reserved;
+    return BSAR_OK;
+}
+
+void bsar_server_destroy(bsar_server* s)
+{
+    if (!s) return;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+        s->cv_work.notify_all();
+    }
+    if (s->worker.joinable()) s->worker.join();
+    {
+        std::lock_guard<std::mutex> lk(s->ctx->mu);
+        cudaSetDevice(s->ctx->device);
+        if (s->run) cudaStreamSynchronize(s->run);
+        if (s->io) cudaStreamSynchronize(s->io);
+        for (auto& kv : s->graphs) cudaGraphExecDestroy(kv.second);
+        for (auto& kv : s->reqs) {
+            kv.second->scene.reset();
+            kv.second->axes.reset();
+            kv.second->image.reset();
+        }
+        s->d_reqs.reset();
+        s->d_tiles.reset();
+        s->d_ntiles.reset();
+        s->d_counter.reset();
+        if (s->h_reqs) cudaFreeHost(s->h_reqs);
+        if (s->h_tiles) cudaFreeHost(s->h_tiles);
+        if (s->h_ntiles) cudaFreeHost(s->h_ntiles);
+        if (s->ev_done) cudaEventDestroy(s->ev_done);
+        if (s->run) cudaStreamDestroy(s->run);
+        if (s->io) cudaStreamDestroy(s->io);
+    }
+    delete s;
+}
+
+}  // extern "C"

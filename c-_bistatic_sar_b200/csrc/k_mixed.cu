@@ -526,31 +526,39 @@ __device__ __forceinline__ double solve_mixed(const DemView& d, const MixedCtx& 
 // ------------------------------- TMA tile staging -----------------------------------
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-__device__ __forceinline__ uint32_t mbar_try_wait(uint32_t bar)
+__device__ __forceinline__ uint32_t mbar_try_wait_parity(uint32_t bar, uint32_t parity)
 {
     uint32_t done;
     asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}\n"
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
         : "=r"(done)
-        : "r"(bar)
+        : "r"(bar), "r"(parity)
         : "memory");
     return done;
 }
 
-// One elected thread loads the tile with a TMA 2-D tiled copy completing on `mbar`;
-// every thread then waits with a bounded spin.  Returns false (and raises *status) if
-// the copy did not complete in time.
-__device__ bool stage_tile(const CUtensorMap* tmap, float* tile, uint64_t* mbar, int i0, int j0, int* status)
+// A copy that missed its deadline may still be in flight: wait for it (bounded) before
+// the CTA's shared memory is released.
+__device__ void drain_tile(uint64_t* mbar, uint32_t parity)
+{
+    const uint32_t bar = smem_u32(mbar);
+    uint32_t done = 0;
+    for (long s = 0; s < kWaitSpins && !done; s++) done = mbar_try_wait_parity(bar, parity);
+}
+
+// Arms `mbar` and has one elected thread load the tile with a TMA 2-D tiled copy that
+// completes on it; every thread then waits (bounded) for the barrier's phase `parity`.
+// Returns false (and raises *status) if the copy did not complete in time.  The caller
+// has initialised the barrier and synchronised the CTA after the previous tile's readers.
+__device__ bool stage_tile(const void* tmap, float* tile, uint64_t* mbar, int i0, int j0, uint32_t parity, int* status)
 {
     const uint32_t bar = smem_u32(mbar);
     if (threadIdx.x == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
         const uint32_t bytes = TI * TJ * sizeof(float);
+        // the tensor map sits in global memory written by host copies (a request slot is
+        // reused by later requests): acquire it for the tensormap proxy before the copy
+        asm volatile("fence.proxy.tensormap::generic.acquire.sys [%0], 128;" ::"l"(reinterpret_cast<uint64_t>(tmap))
+                     : "memory");
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
         asm volatile(
             "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
@@ -558,147 +566,178 @@ __device__ bool stage_tile(const CUtensorMap* tmap, float* tile, uint64_t* mbar,
             : "memory");
     }
     uint32_t done = 0;
-    for (long s = 0; s < kWaitSpins && !done; s++) done = mbar_try_wait(bar);
+    for (long s = 0; s < kWaitSpins && !done; s++) done = mbar_try_wait_parity(bar, parity);
     if (!done && status) atomicExch(status, 1);
     return done != 0;
 }
 
-// A copy that missed its deadline may still be in flight: wait for it (bounded) before
-// the CTA's shared memory is released.
-__device__ void drain_tile(uint64_t* mbar)
+__device__ __forceinline__ MixedCtx req_ctx(const MixedReq& r)
 {
-    const uint32_t bar = smem_u32(mbar);
-    uint32_t done = 0;
-    for (long s = 0; s < kWaitSpins && !done; s++) done = mbar_try_wait(bar);
+    MixedCtx m;
+    m.z32 = r.z32;
+    m.pitch = r.pitch;
+    m.nx = r.a.dem.nx;
+    m.ny = r.a.dem.ny;
+    m.stepx = r.stepx;
+    m.stepy = r.stepy;
+    m.istepx = r.istepx;
+    m.istepy = r.istepy;
+    m.ox = r.ox;
+    m.oy = r.oy;
+    m.idx64 = r.idx64;
+    m.idy64 = r.idy64;
+    return m;
 }
 
-struct MixedExtra {
-    float off_x, off_y;   // mean crossing offset from the voxel (m), tile centring
-    int* status;          // device status word: 1 = a tile copy timed out
-    int use_tile;
-};
-
-}  // namespace
-
-template <int FP16, int WT>
-__global__ void __launch_bounds__(128, 5) k_bp_mixed(BpArgs a, MixedCtx m, MixedExtra ex,
-                                                  const __grid_constant__ CUtensorMap tmap)
+// One voxel of a request over all its pulses (k: index in the request's voxel range;
+// k >= v_count repeats the last voxel without storing it, so whole warps stay active).
+template <int WT>
+__device__ __forceinline__ void voxel_mixed(const BpArgs& a, const MixedCtx& m, const Tile& T, float* table_buf,
+                                            bool fp16, int64_t kk)
 {
-    __shared__ alignas(128) float tile_s[TI * TJ];
-    __shared__ alignas(16) float air_s[4][TBI * TBJ];     // one E-leg table per warp
-    __shared__ alignas(8) uint64_t mbar;
-    float* table_buf = air_s[threadIdx.x >> 5];
-    const int* __restrict__ ref_bin_i = a.ref_bin_i;
-    const float* __restrict__ ref_bin_f = a.ref_bin_f;
     const int np = a.np;
     const float k_bin = (float)(a.fs_eff / a.c);
     const float k_phase = (float)(2.0 * 3.14159265358979323846 / a.lambda);
     const float n1f = (float)a.n1, n2f = (float)a.n2;
     const int64_t nr = a.nr;
-
-    // tile centred on this CTA's voxels plus the scene's mean crossing offset
-    Tile T{tile_s, 0, 0, false};
-    if (ex.use_tile) {
-        const int64_t v0 = a.v_begin + (int64_t)blockIdx.x * blockDim.x;
-        const int64_t vl = min(v0 + (int64_t)blockDim.x, a.v_begin + a.v_count) - 1;
-        const int64_t vm = (v0 + vl) / 2;
-        const double cx = __ldg(a.gx + (int)((vm / a.ny) % a.nx)) + ex.off_x;
-        const double cy = __ldg(a.gy + (int)(vm % a.ny)) + ex.off_y;
-        const int ci = (int)floor((cx - m.ox) / m.stepx), cj = (int)floor((cy - m.oy) / m.stepy);
-        T.i0 = ((ci - TI / 2) >> 2) << 2;      // TMA: x offset a multiple of 4 floats (16 B)
-        T.j0 = cj - TJ / 2;
-        T.ok = stage_tile(&tmap, tile_s, &mbar, T.i0, T.j0, ex.status);
-    }
-
-    // every lane walks the pulses (the warp tables need the full warp); lanes past the
-    // end of the grid repeat the last voxel and do not store it
-    const int64_t kk = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    {
-        const int64_t k = kk < a.v_count ? kk : a.v_count - 1;
-        const int64_t v = a.v_begin + k;
-        const int yi = (int)(v % a.ny);
-        const int xi = (int)((v / a.ny) % a.nx);
-        const int zi = (int)(v / ((int64_t)a.nx * a.ny));
-        const double P[3] = {__ldg(a.gx + xi), __ldg(a.gy + yi), __ldg(a.gz + zi)};
-        const float P32[3] = {(float)(P[0] - m.ox), (float)(P[1] - m.oy), (float)P[2]};
-        float accr = 0.f, acci = 0.f, cmpr = 0.f, cmpi = 0.f;
-        for (int i = 0; i < np; i++) {
-            const double Tx[3] = {__ldg(a.tx + 3 * i), __ldg(a.tx + 3 * i + 1), __ldg(a.tx + 3 * i + 2)};
-            const double Rx[3] = {__ldg(a.rx + 3 * i), __ldg(a.rx + 3 * i + 1), __ldg(a.rx + 3 * i + 2)};
-            const float T32[3] = {(float)(Tx[0] - m.ox), (float)(Tx[1] - m.oy), (float)Tx[2]};
-            const float R32[3] = {(float)(Rx[0] - m.ox), (float)(Rx[1] - m.oy), (float)Rx[2]};
-            // per-pulse legs: n1*r1Tx + n2*r2Tx (Tx -> voxel) + n2*r2Rx + n1*r1Rx (voxel -> Rx);
-            // one solver body serves both legs
-            double L = 0.0;
+    const int64_t k = kk < a.v_count ? kk : a.v_count - 1;
+    const int64_t v = a.v_begin + k;
+    const int yi = (int)(v % a.ny);
+    const int xi = (int)((v / a.ny) % a.nx);
+    const int zi = (int)(v / ((int64_t)a.nx * a.ny));
+    const double P[3] = {__ldg(a.gx + xi), __ldg(a.gy + yi), __ldg(a.gz + zi)};
+    const float P32[3] = {(float)(P[0] - m.ox), (float)(P[1] - m.oy), (float)P[2]};
+    float accr = 0.f, acci = 0.f, cmpr = 0.f, cmpi = 0.f;
+    for (int i = 0; i < np; i++) {
+        const double Tx[3] = {__ldg(a.tx + 3 * i), __ldg(a.tx + 3 * i + 1), __ldg(a.tx + 3 * i + 2)};
+        const double Rx[3] = {__ldg(a.rx + 3 * i), __ldg(a.rx + 3 * i + 1), __ldg(a.rx + 3 * i + 2)};
+        const float T32[3] = {(float)(Tx[0] - m.ox), (float)(Tx[1] - m.oy), (float)Tx[2]};
+        const float R32[3] = {(float)(Rx[0] - m.ox), (float)(Rx[1] - m.oy), (float)Rx[2]};
+        // per-pulse legs: n1*r1Tx + n2*r2Tx (Tx -> voxel) + n2*r2Rx + n1*r1Rx (voxel -> Rx);
+        // one solver body serves both legs
+        double L = 0.0;
 #pragma unroll 1
-            for (int leg = 0; leg < 2; leg++) {
-                // endpoints selected element-wise so they stay in registers
-                const double A[3] = {leg ? P[0] : Tx[0], leg ? P[1] : Tx[1], leg ? P[2] : Tx[2]};
-                const double B[3] = {leg ? Rx[0] : P[0], leg ? Rx[1] : P[1], leg ? Rx[2] : P[2]};
-                const float A32[3] = {leg ? P32[0] : T32[0], leg ? P32[1] : T32[1], leg ? P32[2] : T32[2]};
-                const float B32[3] = {leg ? R32[0] : P32[0], leg ? R32[1] : P32[1], leg ? R32[2] : P32[2]};
-                double dA, dB;
-                L += solve_mixed<WT, true>(a.dem, m, T, table_buf, A, B, A32, B32, leg ? n2f : n1f, leg ? n1f : n2f,
-                                           leg == 0, a.W, dA, dB);
-            }
-            const float dL = (float)(L - __ldg(a.ref_L + i));
-            // fast-time bin: integer anchor + FP32 offset
-            const float t = __ldg(ref_bin_f + i) + dL * k_bin;
-            const float fl = floorf(t);
-            const int64_t lo = (int64_t)__ldg(ref_bin_i + i) + (int64_t)fl;
-            const float q = t - fl;
-            const bool exact = (q == 0.0f);
-            if (lo >= 0 && (lo < nr - 1 || (lo == nr - 1 && exact))) {
-                float s0r, s0i, s1r = 0.f, s1i = 0.f;
-                const int64_t base = (int64_t)i * nr + lo;
-                if constexpr (FP16) {
-                    const float sc = __ldg(a.scale16 + i);
-                    float2 f0 = __half22float2(a.rc16[base]);
-                    s0r = f0.x * sc;
-                    s0i = f0.y * sc;
-                    if (!exact) {
-                        float2 f1 = __half22float2(a.rc16[base + 1]);
-                        s1r = f1.x * sc;
-                        s1i = f1.y * sc;
-                    }
-                } else {
-                    float2 f0 = __ldg(a.rc32 + base);
-                    s0r = f0.x;
-                    s0i = f0.y;
-                    if (!exact) {
-                        float2 f1 = __ldg(a.rc32 + base + 1);
-                        s1r = f1.x;
-                        s1i = f1.y;
-                    }
-                }
-                const float w0 = 1.0f - q;
-                const float vr = exact ? s0r : fmaf(w0, s0r, q * s1r);
-                const float vi = exact ? s0i : fmaf(w0, s0i, q * s1i);
-                // carrier phase: FP64-reduced anchor + FP32 offset, reduced again to [-pi, pi]
-                float ph = __ldg(a.ref_phase + i) + dL * k_phase;
-                const float kk = rintf(ph * 0.15915494309189535f);
-                ph = fmaf(-kk, 6.28318548202514648f, ph);
-                ph = fmaf(-kk, -1.7484555e-7f, ph);
-                float sn, cs;
-                __sincosf(ph, &sn, &cs);
-                const float cr = vr * cs - vi * sn;
-                const float ci = vr * sn + vi * cs;
-                // Kahan-compensated sums
-                float y = cr - cmpr;
-                float tt = accr + y;
-                cmpr = (tt - accr) - y;
-                accr = tt;
-                y = ci - cmpi;
-                tt = acci + y;
-                cmpi = (tt - acci) - y;
-                acci = tt;
-            }
+        for (int leg = 0; leg < 2; leg++) {
+            // endpoints selected element-wise so they stay in registers
+            const double A[3] = {leg ? P[0] : Tx[0], leg ? P[1] : Tx[1], leg ? P[2] : Tx[2]};
+            const double B[3] = {leg ? Rx[0] : P[0], leg ? Rx[1] : P[1], leg ? Rx[2] : P[2]};
+            const float A32[3] = {leg ? P32[0] : T32[0], leg ? P32[1] : T32[1], leg ? P32[2] : T32[2]};
+            const float B32[3] = {leg ? R32[0] : P32[0], leg ? R32[1] : P32[1], leg ? R32[2] : P32[2]};
+            double dA, dB;
+            L += solve_mixed<WT, true>(a.dem, m, T, table_buf, A, B, A32, B32, leg ? n2f : n1f, leg ? n1f : n2f,
+                                       leg == 0, a.W, dA, dB);
         }
-        if (kk < a.v_count)
-            a.out[((int64_t)xi * a.ny + yi) * a.nz + zi] =
-                make_double2((double)accr - (double)cmpr, (double)acci - (double)cmpi);
+        const float dL = (float)(L - __ldg(a.ref_L + i));
+        // fast-time bin: integer anchor + FP32 offset
+        const float t = __ldg(a.ref_bin_f + i) + dL * k_bin;
+        const float fl = floorf(t);
+        const int64_t lo = (int64_t)__ldg(a.ref_bin_i + i) + (int64_t)fl;
+        const float q = t - fl;
+        const bool exact = (q == 0.0f);
+        if (lo >= 0 && (lo < nr - 1 || (lo == nr - 1 && exact))) {
+            float s0r, s0i, s1r = 0.f, s1i = 0.f;
+            const int64_t base = (int64_t)i * nr + lo;
+            if (fp16) {
+                const float sc = __ldg(a.scale16 + i);
+                float2 f0 = __half22float2(a.rc16[base]);
+                s0r = f0.x * sc;
+                s0i = f0.y * sc;
+                if (!exact) {
+                    float2 f1 = __half22float2(a.rc16[base + 1]);
+                    s1r = f1.x * sc;
+                    s1i = f1.y * sc;
+                }
+            } else {
+                float2 f0 = __ldg(a.rc32 + base);
+                s0r = f0.x;
+                s0i = f0.y;
+                if (!exact) {
+                    float2 f1 = __ldg(a.rc32 + base + 1);
+                    s1r = f1.x;
+                    s1i = f1.y;
+                }
+            }
+            const float w0 = 1.0f - q;
+            const float vr = exact ? s0r : fmaf(w0, s0r, q * s1r);
+            const float vi = exact ? s0i : fmaf(w0, s0i, q * s1i);
+            // carrier phase: FP64-reduced anchor + FP32 offset, reduced again to [-pi, pi]
+            float ph = __ldg(a.ref_phase + i) + dL * k_phase;
+            const float kr = rintf(ph * 0.15915494309189535f);
+            ph = fmaf(-kr, 6.28318548202514648f, ph);
+            ph = fmaf(-kr, -1.7484555e-7f, ph);
+            float sn, cs;
+            __sincosf(ph, &sn, &cs);
+            const float cr = vr * cs - vi * sn;
+            const float ci = vr * sn + vi * cs;
+            // Kahan-compensated sums
+            float y = cr - cmpr;
+            float tt = accr + y;
+            cmpr = (tt - accr) - y;
+            accr = tt;
+            y = ci - cmpi;
+            tt = acci + y;
+            cmpi = (tt - acci) - y;
+            acci = tt;
+        }
     }
-    if (ex.use_tile && !T.ok) drain_tile(&mbar);
+    if (kk < a.v_count)
+        a.out[((int64_t)xi * a.ny + yi) * a.nz + zi] =
+            make_double2((double)accr - (double)cmpr, (double)acci - (double)cmpi);
+}
+
+}  // namespace
+
+// Persistent mixed back-projection.  Every CTA takes work items -- one request and 128
+// consecutive voxels of it -- from the batch's list through an atomic counter until the
+// list is exhausted, so tiles of several requests share one launch.  The 128 voxels of a
+// work item are the same 128 a one-request launch gives a CTA, so a voxel's arithmetic
+// (warp tables, DEM tile, sums) does not depend on what else is in the batch.
+template <int WT>
+__global__ void __launch_bounds__(128, 5) k_bp_mixed(MixedBatch b)
+{
+    __shared__ alignas(128) float tile_s[TI * TJ];
+    __shared__ alignas(16) float air_s[4][TBI * TBJ];     // one E-leg table per warp
+    __shared__ alignas(8) uint64_t mbar;
+    __shared__ int2 work;
+    float* table_buf = air_s[threadIdx.x >> 5];
+    const int ntiles = b.ntiles_dev ? *b.ntiles_dev : b.ntiles;
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    uint32_t parity = 0;
+    bool copy_pending = false;     // a tile copy that timed out may still land
+    for (;;) {
+        __syncthreads();           // previous work item done (tile, table, `work`)
+        if (threadIdx.x == 0) {
+            const int t = atomicAdd(b.counter, 1);
+            work = (t < ntiles) ? (b.tiles ? b.tiles[t] : make_int2(0, t)) : make_int2(-1, -1);
+        }
+        __syncthreads();
+        const int2 w = work;
+        if (w.x < 0) break;
+        const MixedReq& R = b.reqs[w.x];
+        const BpArgs& a = R.a;
+        const MixedCtx m = req_ctx(R);
+        Tile T{tile_s, 0, 0, false};
+        if (R.use_tile && !copy_pending) {
+            // DEM tile centred on this work item's voxels plus the mean crossing offset
+            const int64_t v0 = a.v_begin + (int64_t)w.y * 128;
+            const int64_t vl = min(v0 + 128, a.v_begin + a.v_count) - 1;
+            const int64_t vm = (v0 + vl) / 2;
+            const double cx = __ldg(a.gx + (int)((vm / a.ny) % a.nx)) + R.off_x;
+            const double cy = __ldg(a.gy + (int)(vm % a.ny)) + R.off_y;
+            const int ci = (int)floor((cx - m.ox) / m.stepx), cj = (int)floor((cy - m.oy) / m.stepy);
+            T.i0 = ((ci - TI / 2) >> 2) << 2;      // TMA: x offset a multiple of 4 floats (16 B)
+            T.j0 = cj - TJ / 2;
+            T.ok = stage_tile(R.tmap, tile_s, &mbar, T.i0, T.j0, parity, b.status);
+            parity ^= 1u;
+            copy_pending = !T.ok;
+        }
+        voxel_mixed<WT>(a, m, T, table_buf, R.fp16 != 0, (int64_t)w.y * 128 + threadIdx.x);
+    }
+    if (copy_pending) drain_tile(&mbar, parity ^ 1u);
 }
 
 static MixedCtx mixed_ctx(const DemView& d, int pitch)
@@ -747,40 +786,27 @@ cudaError_t launch_refraction_mixed(const DemView& d, int pitch, const double* p
     return cudaGetLastError();
 }
 
-template <int FP16, int WT>
-static void launch_w(const BpArgs& a, const MixedCtx& m, const MixedExtra& ex, const CUtensorMap& tmap, int blocks,
-                     cudaStream_t st)
+int mixed_grid_ctas()
 {
-    k_bp_mixed<FP16, WT><<<blocks, 128, 0, st>>>(a, m, ex, tmap);
-}
-
-template <int FP16>
-static void launch_fp(const BpArgs& a, const MixedCtx& m, const MixedExtra& ex, const CUtensorMap& tmap, int blocks,
-                      cudaStream_t st)
-{
-    switch (a.W) {
-    case 3: launch_w<FP16, 3>(a, m, ex, tmap, blocks, st); break;
-    case 6: launch_w<FP16, 6>(a, m, ex, tmap, blocks, st); break;
-    case 12: launch_w<FP16, 12>(a, m, ex, tmap, blocks, st); break;
-    default: launch_w<FP16, 0>(a, m, ex, tmap, blocks, st); break;
+    static int ctas = 0;
+    if (!ctas) {
+        int dev = 0, sms = 148, per = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_bp_mixed<6>, 128, 0);
+        ctas = sms * (per > 0 ? per : 1);
     }
+    return ctas;
 }
 
-cudaError_t launch_bp_mixed(const BpArgs& a, const MixedLaunch& ml, int legs, int fp16, cudaStream_t st)
+cudaError_t launch_bp_mixed(const MixedBatch& b, int W, int grid, cudaStream_t st)
 {
-    // the mean-over-pulses legs of the reference (proc_test_script.cpp:518-548) are served
-    // by the FP64 form only
-    if (legs == 0) return cudaErrorNotSupported;
-    MixedCtx m = mixed_ctx(a.dem, ml.pitch);
-    MixedExtra ex{ml.off_x, ml.off_y, ml.status, ml.tmap ? 1 : 0};
-    CUtensorMap tmap{};
-    if (ml.tmap) tmap = *reinterpret_cast<const CUtensorMap*>(ml.tmap);
-    int64_t blocks64 = (a.v_count + 127) / 128;
-    int blocks = (int)(blocks64 < 1 ? 1 : (blocks64 > (int64_t)1 << 30 ? (int64_t)1 << 30 : blocks64));
-    if (fp16)
-        launch_fp<1>(a, m, ex, tmap, blocks, st);
-    else
-        launch_fp<0>(a, m, ex, tmap, blocks, st);
+    switch (W) {
+    case 3: k_bp_mixed<3><<<grid, 128, 0, st>>>(b); break;
+    case 6: k_bp_mixed<6><<<grid, 128, 0, st>>>(b); break;
+    case 12: k_bp_mixed<12><<<grid, 128, 0, st>>>(b); break;
+    default: k_bp_mixed<0><<<grid, 128, 0, st>>>(b); break;
+    }
     return cudaGetLastError();
 }
 

@@ -11,8 +11,15 @@
 // src/interpolation.cpp:4-51 runs as the epilogue, reading neighbours from shared
 // memory and writing the upsampled pulse in the requested storage type.
 //
+// Pulses longer than one CTA's shared memory holds (FP64 above 8192, FP32 above 16384
+// samples) run on a thread-block cluster of C = 2..8 CTAs: CTA r holds elements
+// [r*M, (r+1)*M), M = P/C.  The radix-2 stages whose span reaches M pair elements of two
+// CTAs and exchange them through distributed shared memory; every butterfly performs
+// the same operations as the one-CTA transform, so both give identical bits.
+//
 // Compiled with --fmad=false: the Hermite epilogue (and the standalone spline kernel)
 // reproduce the reference's FP64 results bit for bit.
+#include <cooperative_groups.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
@@ -307,15 +314,292 @@ __global__ void k_spline(const double2* __restrict__ in, int64_t n, int64_t batc
     }
 }
 
+
+// ---------------------------------------------------------------------------------
+// Cluster-split transforms (P = C * M, CTA r of the cluster holds x[r*M .. r*M+M)).
+// ---------------------------------------------------------------------------------
+namespace cg = cooperative_groups;
+
+constexpr int kClThreads = 1024;
+template <typename R> struct ClPer;                       // elements per thread at M max
+template <> struct ClPer<double> { static constexpr int v = 8; };    // M <= 8192  (128 KB)
+template <> struct ClPer<float> { static constexpr int v = 16; };    // M <= 16384 (128 KB)
+
+// One radix-2 stage of span h >= M: each CTA updates its own M elements from their
+// partners in CTA r ^ (h / M).  dit = 0: DIF butterfly, dit = 1: DIT butterfly.
+template <typename R, typename V>
+__device__ __forceinline__ void cl_stage(V* x, int P, int s, int logM, const V* __restrict__ tw, int dit,
+                                         const cg::cluster_group& cl)
+{
+    constexpr int kPer = ClPer<R>::v;
+    const int M = 1 << logM;
+    const unsigned r = cl.block_rank();
+    const int base = (int)(r << logM);
+    const int h = 1 << s;
+    const int tstride = P >> (s + 1);
+    const V* peer = cl.map_shared_rank(x, r ^ (unsigned)(h >> logM));
+    V nv[kPer];
+    cl.sync();                                    // every CTA's previous stage is written
+#pragma unroll
+    for (int j = 0; j < kPer; j++) {
+        const int l = threadIdx.x + j * kClThreads;
+        if (l < M) {
+            const int i = base + l;
+            const V a = x[l], c = peer[l];            // own element, partner element
+            const V w = __ldg(tw + (i & (h - 1)) * tstride);
+            const bool lo = (i & h) == 0;             // i is the butterfly's first index
+            if (!dit)
+                nv[j] = lo ? cadd(a, c) : cmul(csub(c, a), w);
+            else
+                nv[j] = lo ? cadd(a, cmul(c, w)) : csub(c, cmul(a, w));
+        }
+    }
+    cl.sync();                                    // all partner reads are done
+#pragma unroll
+    for (int j = 0; j < kPer; j++) {
+        const int l = threadIdx.x + j * kClThreads;
+        if (l < M) x[l] = nv[j];
+    }
+}
+
+// DIF over the whole cluster: natural order in, bit-reversed order out (global indices).
+template <typename R, typename V>
+__device__ void fft_dif_cl(V* x, int P, int logP, int logM, const V* __restrict__ tw, const cg::cluster_group& cl)
+{
+    for (int s = logP - 1; s >= logM; s--) cl_stage<R>(x, P, s, logM, tw, 0, cl);
+    __syncthreads();
+    const int M = 1 << logM;
+    for (int s = logM - 1; s >= 0; s--) {
+        const int h = 1 << s;
+        const int tstride = P >> (s + 1);
+        for (int b = threadIdx.x; b < (M >> 1); b += blockDim.x) {
+            int k = b & (h - 1);
+            int i0 = ((b >> s) << (s + 1)) + k;
+            int i1 = i0 + h;
+            V a = x[i0], c = x[i1];
+            x[i0] = cadd(a, c);
+            x[i1] = cmul(csub(a, c), __ldg(tw + k * tstride));
+        }
+        __syncthreads();
+    }
+}
+
+// DIT over the whole cluster: bit-reversed order in, natural order out.  Ends with a
+// cluster barrier, so every CTA may read any element afterwards.
+template <typename R, typename V>
+__device__ void fft_dit_cl(V* x, int P, int logP, int logM, const V* __restrict__ tw, const cg::cluster_group& cl)
+{
+    const int M = 1 << logM;
+    for (int s = 0; s < logM; s++) {
+        const int h = 1 << s;
+        const int tstride = P >> (s + 1);
+        for (int b = threadIdx.x; b < (M >> 1); b += blockDim.x) {
+            int k = b & (h - 1);
+            int i0 = ((b >> s) << (s + 1)) + k;
+            int i1 = i0 + h;
+            V t = cmul(x[i1], __ldg(tw + k * tstride));
+            V a = x[i0];
+            x[i0] = cadd(a, t);
+            x[i1] = csub(a, t);
+        }
+        __syncthreads();
+    }
+    for (int s = logM; s < logP; s++) cl_stage<R>(x, P, s, logM, tw, 1, cl);
+    cl.sync();
+}
+
+template <typename V>
+__device__ __forceinline__ V cl_load(V* x, int j, int logM, const cg::cluster_group& cl)
+{
+    const V* q = cl.map_shared_rank(x, (unsigned)(j >> logM));
+    return q[j & ((1 << logM) - 1)];
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kClThreads, 1)
+    k_ref_spectrum_cl(const double2* __restrict__ ref, int nref, int P, int logP, int logM,
+                      const typename C2<R>::T* __restrict__ tw, int correlate, typename C2<R>::T* __restrict__ spec)
+{
+    using V = typename C2<R>::T;
+    cg::cluster_group cl = cg::this_cluster();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V* x = reinterpret_cast<V*>(smem_raw);
+    const int M = 1 << logM;
+    const int base = (int)(cl.block_rank() << logM);
+    for (int l = threadIdx.x; l < M; l += blockDim.x) {
+        V v;
+        const int i = base + l;
+        if (i < nref) { double2 d = ref[i]; v.x = (R)d.x; v.y = (R)d.y; } else { v.x = 0; v.y = 0; }
+        x[l] = v;
+    }
+    fft_dif_cl<R>(x, P, logP, logM, tw, cl);
+    for (int l = threadIdx.x; l < M; l += blockDim.x) spec[base + l] = correlate ? x[l] : cconj(x[l]);
+    cl.sync();
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kClThreads, 1)
+    k_pulse_compress_cl(const double2* __restrict__ in, int ns, int P, int logP, int logM,
+                        const typename C2<R>::T* __restrict__ tw, const typename C2<R>::T* __restrict__ spec,
+                        int n_keep, int factor, int out_kind, double2* __restrict__ out64, float2* __restrict__ out32,
+                        __half2* __restrict__ out16, float* __restrict__ scale16)
+{
+    using V = typename C2<R>::T;
+    cg::cluster_group cl = cg::this_cluster();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V* x = reinterpret_cast<V*>(smem_raw);
+    __shared__ float red[32];
+    const int C = (int)cl.num_blocks();
+    const unsigned r = cl.block_rank();
+    const int M = 1 << logM;
+    const int base = (int)(r << logM);
+    const int64_t p = blockIdx.x / C;
+    const double2* __restrict__ src = in + p * (int64_t)ns;
+    for (int l = threadIdx.x; l < M; l += blockDim.x) {
+        V v;
+        const int i = base + l;
+        if (i < ns) { double2 d = __ldg(src + i); v.x = (R)d.x; v.y = (R)d.y; } else { v.x = 0; v.y = 0; }
+        x[l] = v;
+    }
+    fft_dif_cl<R>(x, P, logP, logM, tw, cl);
+    for (int l = threadIdx.x; l < M; l += blockDim.x) x[l] = cmul(cconj(x[l]), __ldg(spec + base + l));
+    __syncthreads();
+    fft_dit_cl<R>(x, P, logP, logM, tw, cl);
+    const R invP = (R)1 / (R)P;
+    for (int l = threadIdx.x; l < M; l += blockDim.x) {
+        V v = x[l];
+        v.x = v.x * invP;
+        v.y = -v.y * invP;
+        x[l] = v;
+    }
+    cl.sync();
+    if (factor <= 0) {
+        double2* dst = out64 + p * (int64_t)n_keep;
+        for (int l = threadIdx.x; l < M; l += blockDim.x)
+            if (base + l < n_keep) dst[base + l] = make_double2((double)x[l].x, (double)x[l].y);
+        cl.sync();
+        return;
+    }
+    const int64_t n = n_keep;
+    const int64_t nout = n * factor;
+    float scale = 1.0f;
+    if (out_kind == 2) {
+        float m = 0.0f;
+        for (int l = threadIdx.x; l < M; l += blockDim.x)
+            if (base + l < n) m = fmaxf(m, fmaxf(fabsf((float)x[l].x), fabsf((float)x[l].y)));
+        for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            m = (threadIdx.x < (blockDim.x >> 5)) ? red[threadIdx.x] : 0.0f;
+            for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+            if (threadIdx.x == 0) red[0] = m;
+        }
+        cl.sync();
+        m = 0.0f;
+        for (int q = 0; q < C; q++) m = fmaxf(m, *cl.map_shared_rank(&red[0], (unsigned)q));
+        scale = (m > 0.0f) ? m / 16384.0f : 1.0f;
+        if (r == 0 && threadIdx.x == 0) scale16[p] = scale;
+    }
+    const float inv_scale = 1.0f / scale;
+    const int64_t chunk = (nout + C - 1) / C;
+    const int64_t o_end = min(nout, (int64_t)(r + 1) * chunk);
+    for (int64_t o = (int64_t)r * chunk + threadIdx.x; o < o_end; o += blockDim.x) {
+        Hermite H = hermite_at(o, n, factor);
+        const int i = (int)H.idx;
+        V pm1 = cl_load(x, i > 0 ? i - 1 : 0, logM, cl), p0 = cl_load(x, i, logM, cl), p1 = cl_load(x, i + 1, logM, cl);
+        V p2 = cl_load(x, i + 2 < n ? i + 2 : (int)n - 1, logM, cl);
+        double re = hermite_comp(H, n, (double)pm1.x, (double)p0.x, (double)p1.x, (double)p2.x);
+        double im = hermite_comp(H, n, (double)pm1.y, (double)p0.y, (double)p1.y, (double)p2.y);
+        int64_t dst = p * nout + o;
+        if (out_kind == 0)
+            out64[dst] = make_double2(re, im);
+        else if (out_kind == 1)
+            out32[dst] = make_float2((float)re, (float)im);
+        else
+            out16[dst] = __floats2half2_rn((float)re * inv_scale, (float)im * inv_scale);
+    }
+    cl.sync();                                    // peers may still read this CTA's samples
+}
+
+__global__ void __launch_bounds__(kClThreads, 1)
+    k_fft_rows_cl(double2* __restrict__ data, int P, int logP, int logM, const double2* __restrict__ tw, int inverse)
+{
+    cg::cluster_group cl = cg::this_cluster();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* x = reinterpret_cast<double2*>(smem_raw);
+    const int C = (int)cl.num_blocks();
+    const int M = 1 << logM;
+    const int base = (int)(cl.block_rank() << logM);
+    double2* row = data + (int64_t)(blockIdx.x / C) * P;
+    for (int l = threadIdx.x; l < M; l += blockDim.x) {
+        double2 v = row[base + l];
+        if (inverse) v.y = -v.y;
+        x[l] = v;
+    }
+    fft_dif_cl<double>(x, P, logP, logM, tw, cl);
+    cl.sync();
+    for (int l = threadIdx.x; l < M; l += blockDim.x) {
+        double2 v = cl_load(x, (int)brev_n((unsigned)(base + l), logP), logM, cl);
+        if (inverse) {
+            v.x = v.x / (double)P;
+            v.y = -v.y / (double)P;
+        }
+        row[base + l] = v;
+    }
+    cl.sync();
+}
+
 // ------------------------------- launchers ------------------------------------------
 static int fft_threads(int P) { return P >= 1024 ? 512 : (P >= 64 ? P / 2 : 32); }
 
 template <typename R>
 size_t fft_smem_bytes(int P) { return (size_t)P * sizeof(typename C2<R>::T); }
 
+// Cluster size for a P-point transform: 1 while one CTA holds it, else the smallest
+// power of two whose per-CTA share fits (ClPer * kClThreads elements).
+static int cluster_size(int P, int real_bytes)
+{
+    const int mmax = real_bytes == 8 ? ClPer<double>::v * kClThreads : ClPer<float>::v * kClThreads;
+    int C = 1;
+    while (P / C > mmax) C *= 2;
+    return C;
+}
+
+int64_t fft_max_len(int real_bytes) { return 8LL * (real_bytes == 8 ? ClPer<double>::v : ClPer<float>::v) * kClThreads; }
+
+template <typename K, typename... Args>
+static cudaError_t launch_cluster(K kernel, int64_t clusters, int C, size_t smem, cudaStream_t st, Args... args)
+{
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(clusters * C), 1, 1);
+    cfg.blockDim = dim3(kClThreads, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)C;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 cudaError_t launch_ref_spectrum(const double2* ref, int nref, int P, int logP, const void* tw,
                                 int correlate, void* spec, int real_bytes, cudaStream_t st)
 {
+    const int C = cluster_size(P, real_bytes);
+    if (C > 1) {
+        const int logM = logP - __builtin_ctz(C);
+        if (real_bytes == 8)
+            return launch_cluster(k_ref_spectrum_cl<double>, 1, C, fft_smem_bytes<double>(P >> (logP - logM)), st,
+                                  ref, nref, P, logP, logM, (const double2*)tw, correlate, (double2*)spec);
+        return launch_cluster(k_ref_spectrum_cl<float>, 1, C, fft_smem_bytes<float>(P >> (logP - logM)), st, ref,
+                              nref, P, logP, logM, (const float2*)tw, correlate, (float2*)spec);
+    }
     if (real_bytes == 8) {
         size_t sm = fft_smem_bytes<double>(P);
         cudaFuncSetAttribute(k_ref_spectrum<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -332,6 +616,18 @@ cudaError_t launch_ref_spectrum(const double2* ref, int nref, int P, int logP, c
 
 cudaError_t launch_pulse_compress(const PulseArgs& a, cudaStream_t st)
 {
+    const int C = cluster_size(a.P, a.real_bytes);
+    if (C > 1) {
+        const int logM = a.logP - __builtin_ctz(C);
+        const int M = 1 << logM;
+        if (a.real_bytes == 8)
+            return launch_cluster(k_pulse_compress_cl<double>, a.batch, C, fft_smem_bytes<double>(M), st, a.in, a.ns,
+                                  a.P, a.logP, logM, (const double2*)a.tw, (const double2*)a.spec, a.n_keep, a.factor,
+                                  a.out_kind, a.out64, a.out32, a.out16, a.scale16);
+        return launch_cluster(k_pulse_compress_cl<float>, a.batch, C, fft_smem_bytes<float>(M), st, a.in, a.ns, a.P,
+                              a.logP, logM, (const float2*)a.tw, (const float2*)a.spec, a.n_keep, a.factor,
+                              a.out_kind, a.out64, a.out32, a.out16, a.scale16);
+    }
     if (a.real_bytes == 8) {
         size_t sm = fft_smem_bytes<double>(a.P);
         cudaFuncSetAttribute(k_pulse_compress<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -351,6 +647,12 @@ cudaError_t launch_pulse_compress(const PulseArgs& a, cudaStream_t st)
 cudaError_t launch_fft_rows(double2* data, int64_t batch, int P, int logP, const double2* tw, int inverse,
                             cudaStream_t st)
 {
+    const int C = cluster_size(P, 8);
+    if (C > 1) {
+        const int logM = logP - __builtin_ctz(C);
+        return launch_cluster(k_fft_rows_cl, batch, C, fft_smem_bytes<double>(1 << logM), st, data, P, logP, logM, tw,
+                              inverse);
+    }
     size_t sm = (size_t)P * sizeof(double2);
     cudaFuncSetAttribute(k_fft_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     k_fft_rows<<<(unsigned)batch, fft_threads(P), sm, st>>>(data, P, logP, tw, inverse);

@@ -32,12 +32,19 @@ struct PulseArgs {
 cudaError_t launch_ref_spectrum(const double2* ref, int nref, int P, int logP, const void* tw, int correlate,
                                 void* spec, int real_bytes, cudaStream_t st);
 cudaError_t launch_pulse_compress(const PulseArgs& a, cudaStream_t st);
+// longest transform the FFT launchers take (a cluster of up to 8 CTAs)
+int64_t fft_max_len(int real_bytes);
 cudaError_t launch_fft_rows(double2* data, int64_t batch, int P, int logP, const double2* tw, int inverse,
                             cudaStream_t st);
 cudaError_t launch_spline(const double2* in, int64_t n, int64_t batch, int factor, double2* out,
                           cudaStream_t st);
 cudaError_t launch_upsample_store(const double2* in, int64_t n, int64_t batch, int factor, int out_kind, float2* out32,
                                   __half2* out16, float* scale16, cudaStream_t st);
+
+cudaError_t launch_echo_synth(const DemView& d, const double* tx, const double* rx, int np, const double* spos,
+                              const double* samp, int nscat, double n1, double n2, int W, double c, double fc,
+                              double fs, double f0, double f1, double T, int nsamp, double sigma, uint64_t seed,
+                              double* tau, double2* carrier, double2* raw, cudaStream_t st);
 
 // ------------------------------- Fermat (FP64) ---------------------------------------
 cudaError_t launch_dem_elevation(const DemView& d, const double* xy, int64_t n, double* z, cudaStream_t st);
@@ -78,17 +85,38 @@ struct BpArgs {
 constexpr int kMixedTileI = 68;
 constexpr int kMixedTileJ = 64;
 
-struct MixedLaunch {
-    int pitch;            // row pitch (floats) of the FP32 DEM copy; a multiple of 4
-    const void* tmap;     // CUtensorMap of the FP32 DEM (box kMixedTileI x kMixedTileJ), or null
+// One image-formation request of the mixed kernel, as it sits in device memory: the
+// back-projection arguments, the FP32 DEM view and the tensor map of that DEM.
+struct alignas(64) MixedReq {
+    alignas(64) unsigned char tmap[128];   // CUtensorMap of the FP32 DEM (box kMixedTileI x kMixedTileJ)
+    BpArgs a;
+    const float* z32;     // pitch-padded FP32 heights, z32[j * pitch + i]
+    int pitch;            // row pitch (floats), a multiple of 4
+    int use_tile;         // tmap valid: stage DEM tiles with TMA
+    int fp16;             // samples stored FP16 complex + scale (else complex64)
+    int pad;
+    float stepx, stepy, istepx, istepy;
+    double ox, oy;        // origin of the FP32 frame (first DEM node)
+    double idx64, idy64;  // 1 / spacing
     float off_x, off_y;   // mean crossing offset from the voxel, metres (tile centring)
-    int* status;          // device status word (1 = a tile copy timed out)
+};
+
+// A batch of the persistent mixed kernel: `ntiles` work items (request index, tile of 128
+// voxels in the request's flat voxel order); tiles == null means request 0, tiles 0..n-1.
+struct MixedBatch {
+    const MixedReq* reqs;
+    const int2* tiles;
+    const int* ntiles_dev;   // if non-null, the tile count is read on the device
+    int ntiles;
+    int* counter;            // zeroed before the launch
+    int* status;             // device status word (1 = a tile copy timed out)
 };
 
 cudaError_t launch_bp_plain(const BpArgs& a, int solver, int legs, cudaStream_t st);
 cudaError_t launch_refraction_mixed(const DemView& d, int pitch, const double* p1, const double* p2, int64_t n,
                                     double n1, double n2, int W, double* out, cudaStream_t st);
-cudaError_t launch_bp_mixed(const BpArgs& a, const MixedLaunch& ml, int legs, int fp16, cudaStream_t st);
+cudaError_t launch_bp_mixed(const MixedBatch& b, int W, int grid, cudaStream_t st);
+int mixed_grid_ctas();   // persistent grid size (SMs x resident CTAs)
 cudaError_t launch_ref_ranges(const DemView& d, const double* tx, const double* rx, int np, const double* center,
                               double n1, double n2, int W, double lambda, double bin_per_m, double* ref_L,
                               float* ref_phase, int* ref_bin_i, float* ref_bin_f, double* offsets, cudaStream_t st);

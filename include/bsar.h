@@ -175,6 +175,21 @@ typedef struct bsar_scene_desc {
 bsar_status bsar_scene_upload(bsar_ctx* ctx, const bsar_scene_desc* desc, bsar_scene_id* out);
 bsar_status bsar_scene_release(bsar_ctx* ctx, bsar_scene_id scene);
 
+/* Echo synthesis on the device (the simulator's processRawData, src/raw_data_processing.cpp:
+ * 292-421, at the exact fractional delay): a resident raw scene is made from desc (whose
+ * `samples` is ignored) and n_scat point scatterers (positions n x 3, amplitudes n).  Per
+ * pulse and scatterer the FP64 Newton Fermat solve gives the two-way optical path L; the
+ * pulse is sum_s a_s exp(-j 2 pi fc L/c) chirp(t - L/c) with the chirp centred on the
+ * delay, plus complex Gaussian noise of variance Nc / 10^(snr_db/10) per sample (Nc the
+ * chirp length; a non-finite snr_db adds none) drawn from a counter-based generator
+ * seeded by `seed`. */
+bsar_status bsar_scene_synthesize(bsar_ctx* ctx, const bsar_scene_desc* desc, const double* scat_pos,
+                                  const double* scat_amp, int64_t n_scat, double snr_db, uint64_t seed,
+                                  bsar_scene_id* out);
+
+/* Copy a scene's raw (or given compressed) pulses, Np x Ns complex, to the host. */
+bsar_status bsar_scene_read_samples(bsar_ctx* ctx, bsar_scene_id scene, double* out);
+
 /* Pulse compression + upsampling of a resident scene, one launch over all pulses:
  * rootData = IFFT(FFT(raw) . conj(FFT(reference))) per pulse (processRawData,
  * src/raw_data_processing.cpp:371-446) followed by the x`upsample` Hermite interpolation
@@ -184,6 +199,10 @@ bsar_status bsar_scene_compress(bsar_ctx* ctx, bsar_scene_id scene, int32_t prec
 
 /* Copy the scene's upsampled FP64 pulses (Np x Ns*upsample) to the host (diagnostics). */
 bsar_status bsar_scene_read_upsampled(bsar_ctx* ctx, bsar_scene_id scene, double* out);
+
+/* Copy the upsampled pulses as stored for `precision` (complex64, or FP16 complex times
+ * the per-pulse scale), widened to complex128 (diagnostics; compresses when needed). */
+bsar_status bsar_scene_read_stored(bsar_ctx* ctx, bsar_scene_id scene, int32_t precision, double* out);
 
 typedef struct bsar_grid {
     int64_t nx, ny, nz;
@@ -212,6 +231,64 @@ bsar_status bsar_backproject(bsar_ctx* ctx, bsar_scene_id scene, const bsar_grid
  * device memory d_image (complex128, same layout); the grid axes are read at the call. */
 bsar_status bsar_backproject_device(bsar_ctx* ctx, bsar_scene_id scene, const bsar_grid* grid,
                                     const bsar_bp_opts* opts, void* d_image);
+
+/* ---------------------------------------------------------------------------------
+ * Serving: image-formation requests of different grids, pulse counts and DEMs are
+ * admitted as they arrive (FIFO) against an HBM budget; each admitted request's scene
+ * stays resident while its voxel tiles (128 voxels each) are packed with other requests'
+ * tiles into one persistent mixed-kernel launch per batch (optionally a replayed CUDA
+ * graph).  Requests that arrive while others run join the next batch.  A voxel's result
+ * does not depend on what else shares its batch.
+ * ------------------------------------------------------------------------------- */
+typedef struct bsar_server bsar_server;
+typedef uint64_t bsar_request_id;
+
+typedef struct bsar_server_opts {
+    uint64_t hbm_budget_bytes;  /* device bytes admitted requests may hold; 0 = 90 % of the
+                                   context's remaining budget                              */
+    int32_t max_inflight;       /* admitted requests at once (1..256; 0 = 64)             */
+    int32_t tiles_per_launch;   /* work items per launch (0 = two waves of resident CTAs) */
+    int32_t use_graph;          /* 1: every launch replays a captured CUDA graph           */
+    int32_t reserved;
+} bsar_server_opts;
+
+typedef struct bsar_request {
+    bsar_scene_desc scene;      /* scene.samples == NULL: echoes synthesised on the device
+                                   from the scatterers below (bsar_scene_synthesize)       */
+    const double* scat_pos;     /* n_scat x 3 */
+    const double* scat_amp;     /* n_scat     */
+    int64_t n_scat;
+    double snr_db;
+    uint64_t seed;
+    bsar_grid grid;
+    bsar_bp_opts opts;          /* precision BSAR_MIXED or BSAR_MIXED_FP16 (Newton, per-pulse) */
+    double* image_out;          /* nx*ny*nz complex128 [x][y][z], written on completion    */
+} bsar_request;
+
+typedef struct bsar_server_stats {
+    uint64_t submitted, completed, failed, launches, tiles;
+    double p50_ms, p99_ms, mean_ms, max_ms;   /* submission -> image on the host */
+    double voxel_pulses;                      /* work of the completed requests   */
+    double busy_s;                            /* first submission -> last completion */
+    uint64_t peak_inflight;                   /* most requests admitted at once  */
+    uint64_t peak_reserved_bytes;             /* most HBM reserved at once       */
+} bsar_server_stats;
+
+/* The server keeps `ctx` for itself until bsar_server_destroy (other calls on the same
+ * context wait for its lock).  Small request arrays (DEM, trajectories, grid, scatterers)
+ * are copied at submission; scene.samples and image_out must stay valid until the
+ * request completes. */
+bsar_status bsar_server_create(bsar_ctx* ctx, const bsar_server_opts* opts, bsar_server** out);
+bsar_status bsar_server_submit(bsar_server* srv, const bsar_request* req, bsar_request_id* out);
+/* Device bytes a request reserves against the server's budget while admitted.  A
+ * request above the whole budget fails with BSAR_ERR_OOM_BUDGET; smaller ones wait. */
+bsar_status bsar_server_estimate(const bsar_request* req, uint64_t* bytes);
+/* done = 1 when the request finished; its status is the return value once done. */
+bsar_status bsar_server_poll(bsar_server* srv, bsar_request_id id, int32_t* done, double* latency_ms);
+/* Waits up to timeout_s (BSAR_ERR_TIMEOUT when it runs out). */
+bsar_status bsar_server_wait(bsar_server* srv, bsar_request_id id, double timeout_s, double* latency_ms);
+bsar_status bsar_server_get_stats(bsar_server* srv, bsar_server_stats* out);
+void bsar_server_destroy(bsar_server* srv);
 
 #ifdef __cplusplus
 }

@@ -27,14 +27,18 @@ def test_spline_rejects_short_pulse(ctx):
         ctx.spline_upsample(np.ones((1, 1), complex), 4)
 
 
-@pytest.mark.parametrize("n", [2, 8, 256, 4096, 8192])
+# 16384..65536 (FP64) run on clusters of 2, 4 and 8 CTAs
+@pytest.mark.parametrize("n", [2, 8, 256, 4096, 8192, 16384, 32768, 65536])
 def test_fft_matches_oracle(ctx, oracle, n):
     rng = np.random.default_rng(n)
     x = rng.normal(size=(3, n)) + 1j * rng.normal(size=(3, n))
     for inv in (False, True):
         g = ctx.fft(x, inverse=inv)
         o = np.stack([oracle.fft(r, inverse=inv) for r in x])
-        assert rel_l2(g, o) < 1e-13
+        # the reference's twiddle recurrence drifts with length; the device uses a table
+        assert rel_l2(g, o) < (1e-13 if n <= 8192 else 1e-12)
+        npy = np.fft.ifft(x, axis=1) if inv else np.fft.fft(x, axis=1)
+        assert rel_l2(g, npy) < 1e-13
 
 
 def test_fft_known_answers(ctx):
@@ -65,6 +69,34 @@ def test_fft_correlate_matches_oracle(ctx, oracle, sc, conj):
     assert rel_l2(g, o) < 1e-12
 
 
+@pytest.mark.parametrize("ns,nref", [(12000, 16384), (16384, 1201), (30000, 2000)])
+def test_fft_correlate_cluster_lengths(ctx, oracle, ns, nref):
+    """Correlations whose padded length needs a 2- or 4-CTA cluster (FP64)."""
+    rng = np.random.default_rng(ns + nref)
+    x = rng.normal(size=(3, ns)) + 1j * rng.normal(size=(3, ns))
+    r = rng.normal(size=nref) + 1j * rng.normal(size=nref)
+    g = ctx.fft_correlate(x, r)
+    o = oracle.fft_correlate(x, r)
+    assert rel_l2(g, o) < 1e-12
+
+
+def test_scene_compress_long_pulses(ctx, oracle):
+    """16384-sample pulses: FP64 on a 2-CTA cluster, FP32 on one CTA, FP16 storage."""
+    spec = S.scaled(S.config_spec(2), n_pulses=6, n_samples=16384, n_scatterers=8)
+    sc = S.make_scene(spec)
+    o = oracle.spline_upsample(oracle.fft_correlate(sc.raw, sc.reference), 4)
+    sid = bsar.upload_scene(ctx, sc)
+    try:
+        got = {}
+        for prec in ("fp64", "mixed", "mixed_fp16"):
+            got[prec] = ctx.scene_read_stored(sid, spec.n_pulses, spec.n_samples * 4, prec)
+    finally:
+        ctx.scene_release(sid)
+    assert rel_l2(got["fp64"], o) < 1e-12
+    assert rel_l2(got["mixed"], o) < 1e-5
+    assert rel_l2(got["mixed_fp16"], o) < 2e-3
+
+
 def test_matched_filter_peak_at_lag_zero(ctx, sc):
     out = ctx.fft_correlate(sc.reference[None, :], sc.reference)
     assert int(np.argmax(np.abs(out[0]))) == 0
@@ -79,3 +111,31 @@ def test_scene_compress_upsample_matches_oracle(ctx, oracle, sc):
         ctx.scene_release(sid)
     o = oracle.spline_upsample(oracle.fft_correlate(sc.raw, sc.reference), 4)
     assert rel_l2(up, o) < 1e-12
+
+
+def test_gpu_echo_synthesis_matches_numpy(ctx):
+    """Noise-free echoes synthesised on the device equal the numpy generator's (same
+    Newton paths, same centred-chirp model) to 1e-9 relative."""
+    spec = S.scaled(S.config_spec(2), n_pulses=16, n_samples=4096, n_scatterers=5, snr_db=np.inf)
+    sc = S.make_scene(spec)
+    sid = bsar.synthesize_scene(ctx, sc)
+    try:
+        raw = ctx.scene_read_samples(sid, spec.n_pulses, spec.n_samples)
+    finally:
+        ctx.scene_release(sid)
+    assert rel_l2(raw, sc.raw) < 1e-9
+
+
+def test_gpu_echo_synthesis_noise_statistics(ctx):
+    spec = S.scaled(S.config_spec(1), n_pulses=64, n_scatterers=0, snr_db=10.0)
+    sc = S.make_scene(spec, with_raw=False)
+    sid = bsar.synthesize_scene(ctx, sc)
+    try:
+        raw = ctx.scene_read_samples(sid, spec.n_pulses, spec.n_samples)
+    finally:
+        ctx.scene_release(sid)
+    nc = int(spec.pulse_T * spec.fs) + 1
+    want = nc / 10.0                        # Nc / SNR
+    got = np.mean(np.abs(raw) ** 2)
+    assert abs(got / want - 1.0) < 0.02
+    assert abs(np.mean(raw)) < 0.05 * np.sqrt(want)

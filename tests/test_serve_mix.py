@@ -1,0 +1,37 @@
+"""The served workload's request generator and arrival stream (host side, no GPU)."""
+import math
+
+import numpy as np
+
+from bsar import scene as S
+
+
+def test_serve_mix_ranges_and_seeding():
+    m = S.serve_mix(256)
+    a = S.serve_mix(256)
+    assert len(m.requests) == 256 and len(m.dems) == 8
+    for r, q in zip(m.requests, a.requests):
+        sp = r.spec
+        assert 21 <= sp.nx <= 161 and sp.ny == sp.nx and sp.nz == (sp.nx + 1) // 2
+        assert 128 <= sp.n_pulses <= 2048
+        assert sp.n_samples in (2048, 4096, 8192, 16384)
+        assert 5 <= sp.n_scatterers <= 50 and len(r.scat_amp) == sp.n_scatterers
+        assert np.all((r.scat_amp >= 0.1) & (r.scat_amp <= 1.0))
+        assert 3.0 <= sp.eps_r <= 9.0 and 0.1 <= sp.dem_sigma <= 0.5
+        assert r.z.shape == (256, 256)
+        assert np.array_equal(r.scat_pos, q.scat_pos) and np.array_equal(r.tx, q.tx)
+    # DEMs are shared objects (resident once), each with its sigma
+    for (x, y, z, er, sg) in m.dems:
+        assert abs(z.std() - sg) < 1e-9
+    assert len({id(r.z) for r in m.requests}) <= 8
+    # log-uniform grid side: the median side is near the geometric mean of the range
+    sides = np.array([r.spec.nx for r in m.requests])
+    assert abs(np.median(sides) - math.sqrt(21 * 161)) < 15
+
+
+def test_poisson_arrivals():
+    t = S.poisson_arrivals(20000, 50.0)
+    assert t[0] == 0.0 and np.all(np.diff(t) >= 0)
+    gaps = np.diff(t)
+    assert abs(gaps.mean() - 1 / 50.0) < 0.02 / 50.0 * 10
+    assert abs(gaps.std() / gaps.mean() - 1.0) < 0.05       # exponential: cv = 1
