@@ -16,6 +16,14 @@ every pulse (one launch), image left in HBM.
           and the reference's own algorithm (grid search, mean legs) in FP64 on the GPU
           over a voxel subset, with the accuracy of the mixed image against FP64
 
+  serving the served mixed workload: 512 image-formation requests (grid side 21-161,
+          128-2048 pulses, 2048-16384 samples, 8 resident fBm DEMs, 5-50 scatterers)
+          through the continuous-batching server (bsar_server_*), arriving as a Poisson
+          stream at 80 % of the capacity measured on a closed burst of the same mix;
+          latency p50 / p99 from submission to image on the host, echoes synthesised on
+          the device at admission; beside it a sample of the same requests run serially
+          in the plain FP64 form
+
 --impl reference times the reference's CPU implementation (its own sources compiled
 under oracle/_ref, OpenMP over the host cores) on a bounded voxel sample of the same
 scene.  Multi-GPU (torchrun): every rank images its own z-slab of the same size (weak
@@ -208,6 +216,91 @@ def cpu_reference_rate(sc, seconds: float, threads: int, use_ref: bool = True):
         f"{nv_total} voxels)"), "per_voxel_s": per_voxel, "pc_s": t_pc, "upsample_s": t_up}
 
 
+def serve_leg(ctx, torch, n_requests: int, burst: int, fp64_sample: int, load: float = 0.8):
+    """Served mixed workload through bsar_server_* (see the module docstring)."""
+    import bsar
+    from bsar import scene as S
+
+    mix = S.serve_mix(n_requests)
+    reqs = mix.requests
+    vp = np.array([r.spec.voxel_pulses for r in reqs], dtype=np.float64)
+    dems = {}
+
+    def submit(srv, i):
+        r = reqs[i]
+        if id(r.z) not in dems:
+            dems[id(r.z)] = bsar.DemArrays(r.x_vec, r.y_vec, r.z)
+        sp = r.spec
+        return srv.submit(dems[id(r.z)], r.tx, r.rx, r.gx, r.gy, r.gz, n_samples=sp.n_samples, scat_pos=r.scat_pos,
+                          scat_amp=r.scat_amp, snr_db=sp.snr_db, seed=sp.seed, upsample=sp.upsample, n1=sp.n1,
+                          n2=sp.n2, c=3e8, fc=sp.fc, fs=sp.fs, chirp_f0=-sp.bandwidth / 2, chirp_f1=sp.bandwidth / 2,
+                          chirp_T=sp.pulse_T, precision="mixed")
+
+    budget = 120 * 10**9
+    out = {"requests": n_requests, "hbm_budget_bytes": budget, "total_voxel_pulses": float(vp.sum())}
+    # closed burst: capacity of the server on this mix
+    burst = min(burst, n_requests)
+    with bsar.Server(ctx, hbm_budget_bytes=budget) as srv:
+        submit(srv, 0)
+        srv.wait(1)                                            # warm-up (graph capture, first admission)
+        t = time.perf_counter()
+        ids = [submit(srv, i) for i in range(burst)]
+        for i in ids:
+            srv.wait(i)
+        dt = time.perf_counter() - t
+    cap_vps = float(vp[:burst].sum()) / dt
+    rate = load * cap_vps / float(vp.mean())                  # requests/s
+    out["capacity"] = {"voxel_pulses_per_s": cap_vps, "requests": burst, "seconds": dt,
+                       "requests_per_s": cap_vps / float(vp.mean())}
+    # open loop: Poisson arrivals at `load` x capacity
+    arrivals = S.poisson_arrivals(n_requests, rate)
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        with bsar.Server(ctx, hbm_budget_bytes=budget) as srv:
+            submit(srv, 0)
+            srv.wait(1)
+            t0 = time.perf_counter()
+            ids = []
+            for i in range(n_requests):
+                d = t0 + arrivals[i] - time.perf_counter()
+                if d > 0:
+                    time.sleep(d)
+                ids.append(submit(srv, i))
+            lat = [srv.wait(i)[1] for i in ids]
+            wall = time.perf_counter() - t0
+            st = srv.stats()
+    lat = np.asarray(lat)
+    out["served"] = {"arrival_rate_per_s": rate, "load": load, "voxel_pulses_per_s": float(vp.sum()) / wall,
+                     "seconds": wall, "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                     "mean_ms": float(lat.mean()), "max_ms": float(lat.max()), "launches": int(st["launches"]),
+                     "tiles": int(st["tiles"]), "peak_inflight": int(st["peak_inflight"]),
+                     "peak_reserved_gb": st["peak_reserved_bytes"] / 1e9, "failed": int(st["failed"])}
+    out["clocks"] = clk.summary()
+    # the same requests one after another in the plain FP64 form (a spread sample)
+    idx = np.linspace(0, n_requests - 1, min(fp64_sample, n_requests)).astype(int)
+    t_fp64 = 0.0
+    t_mixed = 0.0
+    for i in idx:
+        r = reqs[i]
+        for form, acc in (("fp64", "t_fp64"), ("mixed", "t_mixed")):
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            sid = bsar.synthesize_scene(ctx, r)
+            ctx.backproject(sid, r.gx, r.gy, r.gz, solver="newton", legs="per_pulse", precision=form)
+            ctx.scene_release(sid)
+            dt = time.perf_counter() - t
+            if form == "fp64":
+                t_fp64 += dt
+            else:
+                t_mixed += dt
+    vs = float(vp[idx].sum())
+    out["serial_fp64"] = {"voxel_pulses_per_s": vs / t_fp64, "sample_requests": int(len(idx)),
+                          "sample_voxel_pulses": vs, "seconds": t_fp64,
+                          "est_total_seconds": t_fp64 * float(vp.sum()) / vs}
+    out["serial_mixed"] = {"voxel_pulses_per_s": vs / t_mixed, "seconds": t_mixed}
+    out["served_capacity_vs_serial_fp64"] = cap_vps / (vs / t_fp64)
+    return out
+
+
 def run_reference(args):
     """--impl reference: the reference's CPU implementation on the box's host cores."""
     rank = int(os.environ.get("RANK", "0"))
@@ -250,6 +343,10 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=15.0, help="CPU work per reference sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the comparator forms")
+    ap.add_argument("--serve-requests", type=int, default=512, help="requests of the served workload (0: skip)")
+    ap.add_argument("--serve-burst", type=int, default=64, help="requests of the capacity burst")
+    ap.add_argument("--serve-fp64-sample", type=int, default=24, help="requests run serially in FP64")
+    ap.add_argument("--serve-only", action="store_true", help="only the served workload")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -269,6 +366,14 @@ def main():
         dist = dist_mod
 
     import bsar
+
+    if args.serve_only:
+        ctx = bsar.Context(local)
+        res = serve_leg(ctx, torch, args.serve_requests, args.serve_burst, args.serve_fp64_sample)
+        if rank == 0:
+            print(json.dumps({"serving": res}), flush=True)
+        ctx.close()
+        return 0
 
     sc = make_workload(args.config, rank)
     sp = sc.spec
@@ -389,6 +494,11 @@ def main():
         rate, det = cpu_reference_rate(sc, args.ref_seconds, threads)
         cpu = {"value": rate, "unit": UNIT, "cores": det["cores"], "kind": det["kind"], "sample": det["sample"]}
 
+    serving = None
+    if rank == 0 and world == 1 and args.serve_requests > 0:
+        ctx.set_stream(None)
+        serving = serve_leg(ctx, torch, args.serve_requests, args.serve_burst, args.serve_fp64_sample)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -411,6 +521,7 @@ def main():
             "accuracy": acc,
             "clocks": clocks,
             "cpu_baseline": cpu,
+            "serving": serving,
         }
         print(json.dumps(line), flush=True)
     ctx.scene_release(sid)

@@ -82,7 +82,9 @@ void bsar_destroy(bsar_ctx* ctx)
     ctx->status.reset();
     ctx->mixed_req.reset();
     ctx->mixed_counter.reset();
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+    if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
     delete ctx;
 }
 

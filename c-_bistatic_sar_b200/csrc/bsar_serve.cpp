@@ -1,20 +1,23 @@
 // bsar_serve.cpp -- continuous-batching image-formation server (bsar_server_* of bsar.h).
 //
-// One worker thread per server owns the GPU work:
+// One worker thread per server owns the GPU work.  Two batch slots, each with its own
+// stream, pinned staging and device copies, keep up to two batches in flight:
 //
 //   loop:
-//     launch the next batch (async, `run` stream): the persistent mixed kernel over a
-//       fair-share list of (request, 128-voxel tile) work items of every active request,
-//       as a replay of a captured CUDA graph (copy of the request records and the tile
-//       list from pinned staging, zeroed work counter, kernel)
-//     while it runs: admit pending requests FIFO while the HBM budget and the in-flight
-//       slots allow (scene upload or on-device echo synthesis, pulse compression +
-//       upsampling, per-pulse anchors; `io` stream)
-//     wait for the batch (bounded), retire requests whose tiles are all done (image to
-//       the caller's buffer, resources released, latency recorded)
+//     fill every idle batch slot: a fair-share list of (request, 128-voxel tile) work
+//       items of the admitted requests, longest tiles first, launched as a replay of a
+//       captured CUDA graph (request records and tile list copied from pinned staging,
+//       work counter zeroed, persistent mixed kernel)
+//     wait for the older batch (bounded); while it runs, admit pending requests FIFO
+//       as the HBM budget and the in-flight slots allow (scene upload or on-device echo
+//       synthesis, pulse compression + upsampling, per-pulse anchors; `io` stream,
+//       stream-ordered allocations, so admission never waits for a batch)
+//     retire requests whose tiles are all done (image to the caller's buffer,
+//       resources released, latency recorded)
 //
-// Work items are the same 128-voxel groups a one-request launch uses, so every voxel's
-// arithmetic is independent of the batch it runs in.
+// The second batch's CTAs take the SMs the first batch's tail leaves idle.  Work items
+// are the same 128-voxel groups a one-request launch uses, so every voxel's arithmetic
+// is independent of the batch it runs in.
 #include "runtime.hpp"
 
 #include <chrono>
@@ -72,6 +75,19 @@ uint64_t estimate_bytes(const Req& r)
 
 }  // namespace
 
+struct ServeBatch {
+    MixedReq* h_reqs = nullptr;                     // pinned staging
+    int2* h_tiles = nullptr;
+    int* h_ntiles = nullptr;
+    std::unique_ptr<DevBuf> d_reqs, d_tiles, d_ntiles, d_counter;
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev = nullptr;
+    std::map<int, cudaGraphExec_t> graphs;          // per node-scan width W
+    std::vector<std::pair<Req*, int64_t>> items;    // requests in the batch, tiles each
+    bool inflight = false;
+    uint64_t seq = 0;
+};
+
 struct bsar_server {
     bsar_ctx* ctx = nullptr;
     bsar_server_opts opts{};
@@ -85,14 +101,9 @@ struct bsar_server {
     std::vector<Req*> active;                       // admission order
     std::map<uint64_t, std::unique_ptr<Req>> reqs;
     bool slot_used[kMaxSlots] = {};
-    // batch staging (pinned) and device copies
-    MixedReq* h_reqs = nullptr;
-    int2* h_tiles = nullptr;
-    int* h_ntiles = nullptr;
-    std::unique_ptr<DevBuf> d_reqs, d_tiles, d_ntiles, d_counter;
-    cudaStream_t run = nullptr, io = nullptr;
-    cudaEvent_t ev_done = nullptr;
-    std::map<int, cudaGraphExec_t> graphs;         // per node-scan width W
+    ServeBatch batch[2];
+    uint64_t batch_seq = 0;
+    cudaStream_t io = nullptr;
     int grid_ctas = 0, max_tiles = 0;
     // statistics
     std::vector<double> latencies;
@@ -106,19 +117,23 @@ struct bsar_server {
 
 namespace {
 
-// Runs `f` with the context locked and its stream switched to `st`.
-template <typename F> void with_ctx(bsar_server* s, cudaStream_t st, F&& f)
+// Runs `f` with the context locked, its stream switched to `st` and (when `pooled`)
+// device buffers taken from the stream-ordered pool.
+template <typename F> void with_ctx(bsar_server* s, cudaStream_t st, bool pooled, F&& f)
 {
     std::lock_guard<std::mutex> lk(s->ctx->mu);
     cudaStream_t saved = s->ctx->stream;
     s->ctx->stream = st;
+    s->ctx->use_pool = pooled;
     try {
         f();
     } catch (...) {
         s->ctx->stream = saved;
+        s->ctx->use_pool = false;
         throw;
     }
     s->ctx->stream = saved;
+    s->ctx->use_pool = false;
 }
 
 void finish(bsar_server* s, Req* r, bsar_status st, const std::string& err)
@@ -143,7 +158,7 @@ void finish(bsar_server* s, Req* r, bsar_status st, const std::string& err)
 
 void release(bsar_server* s, Req* r)
 {
-    with_ctx(s, s->io, [&] {
+    with_ctx(s, s->io, true, [&] {
         r->scene.reset();
         r->axes.reset();
         r->image.reset();
@@ -154,7 +169,7 @@ void release(bsar_server* s, Req* r)
 // synthesis, pulse compression + upsampling, anchors, device image.
 void admit(bsar_server* s, Req* r)
 {
-    with_ctx(s, s->io, [&] {
+    with_ctx(s, s->io, true, [&] {
         bsar_ctx* ctx = s->ctx;
         bsar_scene_desc d = r->desc;
         const bool synth = d.samples == nullptr;
@@ -210,24 +225,34 @@ void admit(bsar_server* s, Req* r)
     });
 }
 
-// Fair-share batch: equal tile chunks to every active request, oldest first.
-int build_batch(bsar_server* s, int* W_out)
+// Fair-share batch into slot `b`: equal tile chunks to every active request (oldest
+// first), then ordered longest first (a tile's cost follows its request's pulse count)
+// so the persistent kernel's dynamic work counter ends the batch evenly.
+int build_batch(bsar_server* s, ServeBatch& b, int* W_out)
 {
     int n = 0, W = -1;
     bool mixedW = false;
     std::vector<Req*> live;
     for (Req* r : s->active)
         if (r->next_tile < r->ntiles) live.push_back(r);
+    b.items.clear();
     if (live.empty()) return 0;
+    struct Item {
+        int np, slot, tile;
+    };
+    std::vector<Item> list;
+    std::map<Req*, int64_t> per_req;
     const int chunk = std::max(1, s->max_tiles / (int)live.size());
     bool progress = true;
     while (n < s->max_tiles && progress) {
         progress = false;
         for (Req* r : live) {
             int64_t take = std::min<int64_t>({(int64_t)chunk, r->ntiles - r->next_tile, (int64_t)(s->max_tiles - n)});
-            for (int64_t t = 0; t < take; t++) s->h_tiles[n++] = make_int2(r->slot, (int)(r->next_tile + t));
+            for (int64_t t = 0; t < take; t++) list.push_back({r->rec.a.np, r->slot, (int)(r->next_tile + t)});
             if (take > 0) {
+                n += (int)take;
                 r->next_tile += take;
+                per_req[r] += take;
                 progress = true;
                 if (W < 0) W = r->rec.a.W;
                 else if (W != r->rec.a.W) mixedW = true;
@@ -235,110 +260,124 @@ int build_batch(bsar_server* s, int* W_out)
             if (n >= s->max_tiles) break;
         }
     }
-    for (Req* r : s->active) s->h_reqs[r->slot] = r->rec;
-    *s->h_ntiles = n;
+    std::stable_sort(list.begin(), list.end(), [](const Item& x, const Item& y) { return x.np > y.np; });
+    for (int k = 0; k < n; k++) b.h_tiles[k] = make_int2(list[k].slot, list[k].tile);
+    for (Req* r : s->active) b.h_reqs[r->slot] = r->rec;
+    *b.h_ntiles = n;
+    for (Req* r : s->active)
+        if (per_req.count(r)) b.items.push_back({r, per_req[r]});
     *W_out = mixedW ? 0 : W;
     return n;
 }
 
 // Captured graph of one batch launch: staging copies, counter reset, persistent kernel.
-cudaGraphExec_t batch_graph(bsar_server* s, int W)
+cudaGraphExec_t batch_graph(bsar_server* s, ServeBatch& bt, int W)
 {
-    auto it = s->graphs.find(W);
-    if (it != s->graphs.end()) return it->second;
-    MixedBatch b{s->d_reqs->as<MixedReq>(), s->d_tiles->as<int2>(), s->d_ntiles->as<int>(), 0,
-                 s->d_counter->as<int>(), s->ctx->status->as<int>()};
+    auto it = bt.graphs.find(W);
+    if (it != bt.graphs.end()) return it->second;
+    MixedBatch b{bt.d_reqs->as<MixedReq>(), bt.d_tiles->as<int2>(), bt.d_ntiles->as<int>(), 0,
+                 bt.d_counter->as<int>(), s->ctx->status->as<int>()};
     cudaGraph_t g = nullptr;
-    cuda_check(cudaStreamBeginCapture(s->run, cudaStreamCaptureModeThreadLocal), "begin capture");
-    cudaMemcpyAsync(s->d_reqs->p, s->h_reqs, sizeof(MixedReq) * kMaxSlots, cudaMemcpyHostToDevice, s->run);
-    cudaMemcpyAsync(s->d_tiles->p, s->h_tiles, sizeof(int2) * s->max_tiles, cudaMemcpyHostToDevice, s->run);
-    cudaMemcpyAsync(s->d_ntiles->p, s->h_ntiles, sizeof(int), cudaMemcpyHostToDevice, s->run);
-    cudaMemsetAsync(s->d_counter->p, 0, sizeof(int), s->run);
-    cudaError_t le = launch_bp_mixed(b, W, s->grid_ctas, s->run);
-    cudaError_t ce = cudaStreamEndCapture(s->run, &g);
+    cuda_check(cudaStreamBeginCapture(bt.st, cudaStreamCaptureModeThreadLocal), "begin capture");
+    cudaMemcpyAsync(bt.d_reqs->p, bt.h_reqs, sizeof(MixedReq) * kMaxSlots, cudaMemcpyHostToDevice, bt.st);
+    cudaMemcpyAsync(bt.d_tiles->p, bt.h_tiles, sizeof(int2) * s->max_tiles, cudaMemcpyHostToDevice, bt.st);
+    cudaMemcpyAsync(bt.d_ntiles->p, bt.h_ntiles, sizeof(int), cudaMemcpyHostToDevice, bt.st);
+    cudaMemsetAsync(bt.d_counter->p, 0, sizeof(int), bt.st);
+    cudaError_t le = launch_bp_mixed(b, W, s->grid_ctas, bt.st);
+    cudaError_t ce = cudaStreamEndCapture(bt.st, &g);
     cuda_check(le, "batch launch (capture)");
     cuda_check(ce, "end capture");
     cudaGraphExec_t exec = nullptr;
     cuda_check(cudaGraphInstantiate(&exec, g, 0), "graph instantiate");
     cudaGraphDestroy(g);
-    s->graphs[W] = exec;
+    bt.graphs[W] = exec;
     return exec;
 }
 
-void launch_batch(bsar_server* s, int W, int n)
+void launch_batch(bsar_server* s, ServeBatch& bt, int W, int n)
 {
     if (s->opts.use_graph) {
-        cuda_check(cudaGraphLaunch(batch_graph(s, W), s->run), "graph launch");
+        cuda_check(cudaGraphLaunch(batch_graph(s, bt, W), bt.st), "graph launch");
     } else {
-        MixedBatch b{s->d_reqs->as<MixedReq>(), s->d_tiles->as<int2>(), nullptr, n, s->d_counter->as<int>(),
+        MixedBatch b{bt.d_reqs->as<MixedReq>(), bt.d_tiles->as<int2>(), nullptr, n, bt.d_counter->as<int>(),
                      s->ctx->status->as<int>()};
-        cuda_check(cudaMemcpyAsync(s->d_reqs->p, s->h_reqs, sizeof(MixedReq) * kMaxSlots, cudaMemcpyHostToDevice, s->run),
+        cuda_check(cudaMemcpyAsync(bt.d_reqs->p, bt.h_reqs, sizeof(MixedReq) * kMaxSlots, cudaMemcpyHostToDevice, bt.st),
                    "h2d");
-        cuda_check(cudaMemcpyAsync(s->d_tiles->p, s->h_tiles, sizeof(int2) * n, cudaMemcpyHostToDevice, s->run), "h2d");
-        cuda_check(cudaMemsetAsync(s->d_counter->p, 0, sizeof(int), s->run), "memset");
-        cuda_check(launch_bp_mixed(b, W, std::min(n, s->grid_ctas), s->run), "batch launch");
+        cuda_check(cudaMemcpyAsync(bt.d_tiles->p, bt.h_tiles, sizeof(int2) * n, cudaMemcpyHostToDevice, bt.st), "h2d");
+        cuda_check(cudaMemsetAsync(bt.d_counter->p, 0, sizeof(int), bt.st), "memset");
+        cuda_check(launch_bp_mixed(b, W, std::min(n, s->grid_ctas), bt.st), "batch launch");
     }
-    cuda_check(cudaEventRecord(s->ev_done, s->run), "event");
+    cuda_check(cudaEventRecord(bt.ev, bt.st), "event");
+    bt.inflight = true;
+    bt.seq = ++s->batch_seq;
     s->launches++;
     s->tiles += n;
 }
 
-bool wait_batch(bsar_server* s)
+// Admits the oldest pending request if budget and slots allow (server lock held on entry
+// and exit; released around the device work).  Returns true if it took a request.
+bool admit_one(bsar_server* s, std::unique_lock<std::mutex>& lk)
+{
+    if (s->pending.empty() || s->stop) return false;
+    Req* r = s->pending.front();
+    const uint64_t need = estimate_bytes(*r);
+    int slot = -1;
+    for (int k = 0; k < s->opts.max_inflight; k++)
+        if (!s->slot_used[k]) {
+            slot = k;
+            break;
+        }
+    if (slot < 0) return false;
+    if (s->reserved + need > s->budget && !s->active.empty()) return false;
+    s->pending.pop_front();
+    s->slot_used[slot] = true;
+    r->slot = slot;
+    r->reserved = need;
+    s->reserved += need;
+    s->peak_reserved = std::max(s->peak_reserved, s->reserved);
+    lk.unlock();
+    bsar_status st = BSAR_OK;
+    std::string err;
+    try {
+        if (need > s->budget)
+            fail(BSAR_ERR_OOM_BUDGET, "request needs %llu bytes, the server budget is %llu", (unsigned long long)need,
+                 (unsigned long long)s->budget);
+        admit(s, r);
+    } catch (const Error& e) {
+        st = e.status;
+        err = e.msg;
+    } catch (const std::bad_alloc&) {
+        st = BSAR_ERR_OOM_BUDGET;
+        err = "host allocation failed";
+    }
+    if (st != BSAR_OK) release(s, r);
+    lk.lock();
+    if (st == BSAR_OK) {
+        r->state = St::Active;
+        s->active.push_back(r);
+        s->peak_inflight = std::max<uint64_t>(s->peak_inflight, s->active.size());
+    } else {
+        finish(s, r, st, err);
+        s->cv_done.notify_all();
+    }
+    return true;
+}
+
+// Waits (bounded) for batch `bt`, admitting pending requests while it runs.  Lock held
+// on entry and exit.  Returns an empty string, or why the batch failed.
+std::string wait_batch(bsar_server* s, ServeBatch& bt, std::unique_lock<std::mutex>& lk)
 {
     const auto t0 = Clock::now();
     for (;;) {
-        cudaError_t e = cudaEventQuery(s->ev_done);
-        if (e == cudaSuccess) return true;
-        if (e != cudaErrorNotReady) fail(BSAR_ERR_CUDA, "batch: %s", cudaGetErrorString(e));
-        if (std::chrono::duration<double>(Clock::now() - t0).count() > kBatchTimeoutS) return false;
-        std::this_thread::sleep_for(std::chrono::microseconds(50));
-    }
-}
-
-// Admits pending requests while budget and slots allow (server lock held on entry and
-// exit; released around the device work).
-void admit_pending(bsar_server* s, std::unique_lock<std::mutex>& lk)
-{
-    while (!s->pending.empty() && !s->stop) {
-        Req* r = s->pending.front();
-        const uint64_t need = estimate_bytes(*r);
-        int slot = -1;
-        for (int k = 0; k < s->opts.max_inflight; k++)
-            if (!s->slot_used[k]) {
-                slot = k;
-                break;
-            }
-        if (slot < 0) return;
-        if (s->reserved + need > s->budget && !s->active.empty()) return;
-        s->pending.pop_front();
-        s->slot_used[slot] = true;
-        r->slot = slot;
-        r->reserved = need;
-        s->reserved += need;
-        s->peak_reserved = std::max(s->peak_reserved, s->reserved);
-        lk.unlock();
-        bsar_status st = BSAR_OK;
-        std::string err;
-        try {
-            if (need > s->budget) fail(BSAR_ERR_OOM_BUDGET, "request needs %llu bytes, the server budget is %llu",
-                                       (unsigned long long)need, (unsigned long long)s->budget);
-            admit(s, r);
-        } catch (const Error& e) {
-            st = e.status;
-            err = e.msg;
-        } catch (const std::bad_alloc&) {
-            st = BSAR_ERR_OOM_BUDGET;
-            err = "host allocation failed";
-        }
-        if (st != BSAR_OK) release(s, r);
-        lk.lock();
-        if (st == BSAR_OK) {
-            r->state = St::Active;
-            s->active.push_back(r);
-            s->peak_inflight = std::max<uint64_t>(s->peak_inflight, s->active.size());
-        } else {
-            finish(s, r, st, err);
-            s->cv_done.notify_all();
+        cudaError_t e = cudaEventQuery(bt.ev);
+        if (e == cudaSuccess) return std::string();
+        if (e != cudaErrorNotReady) return std::string("batch: ") + cudaGetErrorString(e);
+        if (std::chrono::duration<double>(Clock::now() - t0).count() > kBatchTimeoutS)
+            return "a batch did not finish within its time limit";
+        if (!admit_one(s, lk)) {
+            lk.unlock();
+            std::this_thread::sleep_for(std::chrono::microseconds(50));
+            lk.lock();
         }
     }
 }
@@ -354,7 +393,7 @@ void retire_finished(bsar_server* s, std::unique_lock<std::mutex>& lk)
         bsar_status st = BSAR_OK;
         std::string err;
         try {
-            with_ctx(s, s->io, [&] {
+            with_ctx(s, s->io, true, [&] {
                 cuda_check(cudaMemcpyAsync(r->image_out, r->image->p, r->image->bytes, cudaMemcpyDeviceToHost, s->io),
                            "image d2h");
                 sync(s->ctx);
@@ -374,74 +413,74 @@ void worker_main(bsar_server* s)
 {
     cudaSetDevice(s->ctx->device);
     std::unique_lock<std::mutex> lk(s->mu);
-    while (true) {
-        if (s->stop) break;
-        // 1. next batch
-        int W = 0;
-        const int n = build_batch(s, &W);
-        std::vector<std::pair<Req*, int64_t>> in_batch;
-        if (n > 0) {
-            std::map<int, int64_t> per_slot;
-            for (int k = 0; k < n; k++) per_slot[s->h_tiles[k].x]++;
-            for (Req* r : s->active)
-                if (per_slot.count(r->slot)) in_batch.push_back({r, per_slot[r->slot]});
-            try {
-                with_ctx(s, s->run, [&] { launch_batch(s, W, n); });
-            } catch (const Error& e) {
-                s->fatal = e.msg;
-                break;
+    while (!s->stop) {
+        // 1. fill the idle batch slots
+        try {
+            for (ServeBatch& bt : s->batch) {
+                if (bt.inflight) continue;
+                int W = 0;
+                const int n = build_batch(s, bt, &W);
+                if (n > 0) with_ctx(s, bt.st, false, [&] { launch_batch(s, bt, W, n); });
             }
+        } catch (const Error& e) {
+            s->fatal = e.msg;
+            break;
         }
-        // 2. admit while it runs
-        admit_pending(s, lk);
-        // 3. wait and retire
-        if (n > 0) {
-            lk.unlock();
-            bool ok = false;
-            std::string err;
-            try {
-                ok = wait_batch(s);
-            } catch (const Error& e) {
-                err = e.msg;
-            }
-            lk.lock();
-            if (!ok) {
-                s->fatal = err.empty() ? "a batch did not finish within its time limit" : err;
-                for (auto& p : in_batch) {
-                    s->active.erase(std::find(s->active.begin(), s->active.end(), p.first));
-                    finish(s, p.first, err.empty() ? BSAR_ERR_TIMEOUT : BSAR_ERR_CUDA, s->fatal);
-                }
-                s->cv_done.notify_all();
-                break;
-            }
-            // a bounded device wait that ran out fails this batch's requests
-            std::string serr;
-            try {
-                with_ctx(s, s->run, [&] { check_device_status(s->ctx); });
-            } catch (const Error& e) {
-                serr = e.msg;
-            }
-            for (auto& p : in_batch) {
-                if (!serr.empty()) {
-                    s->active.erase(std::find(s->active.begin(), s->active.end(), p.first));
-                    lk.unlock();
-                    release(s, p.first);
-                    lk.lock();
-                    finish(s, p.first, BSAR_ERR_TIMEOUT, serr);
-                } else {
-                    p.first->done_tiles += p.second;
-                }
-            }
-            if (!serr.empty()) s->cv_done.notify_all();
-            retire_finished(s, lk);
-        } else if (s->pending.empty() || s->active.size() >= (size_t)s->opts.max_inflight) {
-            s->cv_work.wait_for(lk, std::chrono::milliseconds(2));
+        ServeBatch* old = nullptr;
+        for (ServeBatch& bt : s->batch)
+            if (bt.inflight && (!old || bt.seq < old->seq)) old = &bt;
+        if (!old) {
+            // nothing on the device: admit, or sleep until work arrives
+            if (!admit_one(s, lk)) s->cv_work.wait_for(lk, std::chrono::milliseconds(2));
+            continue;
         }
+        // 2. wait for the older batch, admitting meanwhile
+        std::string err = wait_batch(s, *old, lk);
+        if (!err.empty()) {
+            s->fatal = err;
+            break;
+        }
+        old->inflight = false;
+        // a bounded device wait that ran out: drain the other batch, fail both batches' requests
+        std::string serr;
+        try {
+            with_ctx(s, old->st, false, [&] { check_device_status(s->ctx); });
+        } catch (const Error& e) {
+            serr = e.msg;
+        }
+        if (!serr.empty()) {
+            std::vector<Req*> bad;
+            for (auto& p : old->items) bad.push_back(p.first);
+            for (ServeBatch& bt : s->batch)
+                if (bt.inflight) {
+                    std::string e2 = wait_batch(s, bt, lk);
+                    if (!e2.empty()) s->fatal = e2;
+                    bt.inflight = false;
+                    for (auto& p : bt.items) bad.push_back(p.first);
+                }
+            if (!s->fatal.empty()) break;
+            std::sort(bad.begin(), bad.end());
+            bad.erase(std::unique(bad.begin(), bad.end()), bad.end());
+            for (Req* r : bad) {
+                s->active.erase(std::find(s->active.begin(), s->active.end(), r));
+                lk.unlock();
+                release(s, r);
+                lk.lock();
+                finish(s, r, BSAR_ERR_TIMEOUT, serr);
+            }
+            s->cv_done.notify_all();
+            continue;
+        }
+        for (auto& p : old->items) p.first->done_tiles += p.second;
+        old->items.clear();
+        retire_finished(s, lk);
     }
-    // fail whatever is left
-    for (Req* r : s->active) finish(s, r, BSAR_ERR_CUDA, s->fatal.empty() ? "server stopped" : s->fatal);
+    // fail whatever is left (device buffers are released by bsar_server_destroy after
+    // the batch streams are synchronised)
+    const std::string why = s->fatal.empty() ? "server stopped" : s->fatal;
+    for (Req* r : s->active) finish(s, r, BSAR_ERR_CUDA, why);
     s->active.clear();
-    for (Req* r : s->pending) finish(s, r, BSAR_ERR_CUDA, s->fatal.empty() ? "server stopped" : s->fatal);
+    for (Req* r : s->pending) finish(s, r, BSAR_ERR_CUDA, why);
     s->pending.clear();
     s->cv_done.notify_all();
 }
@@ -476,17 +515,28 @@ bsar_status bsar_server_create(bsar_ctx* ctx, const bsar_server_opts* opts, bsar
         s->max_tiles = s->opts.tiles_per_launch > 0 ? s->opts.tiles_per_launch : 2 * s->grid_ctas;
         const uint64_t free_budget = ctx->budget > ctx->used ? ctx->budget - ctx->used : 0;
         s->budget = s->opts.hbm_budget_bytes ? s->opts.hbm_budget_bytes : (uint64_t)(0.9 * (double)free_budget);
-        cuda_check(cudaStreamCreateWithFlags(&s->run, cudaStreamNonBlocking), "stream");
+        if (!ctx->pool) {
+            cudaMemPoolProps pp = {};
+            pp.allocType = cudaMemAllocationTypePinned;
+            pp.location.type = cudaMemLocationTypeDevice;
+            pp.location.id = ctx->device;
+            cuda_check(cudaMemPoolCreate(&ctx->pool, &pp), "memory pool");
+            uint64_t keep = ~0ull;     // keep freed blocks for the next admission
+            cuda_check(cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep), "pool attribute");
+        }
         cuda_check(cudaStreamCreateWithFlags(&s->io, cudaStreamNonBlocking), "stream");
-        cuda_check(cudaEventCreateWithFlags(&s->ev_done, cudaEventDisableTiming), "event");
-        cuda_check(cudaMallocHost((void**)&s->h_reqs, sizeof(MixedReq) * kMaxSlots), "pinned");
-        cuda_check(cudaMallocHost((void**)&s->h_tiles, sizeof(int2) * s->max_tiles), "pinned");
-        cuda_check(cudaMallocHost((void**)&s->h_ntiles, sizeof(int)), "pinned");
-        std::memset(s->h_reqs, 0, sizeof(MixedReq) * kMaxSlots);
-        s->d_reqs = dev_alloc(ctx, sizeof(MixedReq) * kMaxSlots);
-        s->d_tiles = dev_alloc(ctx, sizeof(int2) * s->max_tiles);
-        s->d_ntiles = dev_alloc(ctx, sizeof(int));
-        s->d_counter = dev_alloc(ctx, sizeof(int));
+        for (ServeBatch& bt : s->batch) {
+            cuda_check(cudaStreamCreateWithFlags(&bt.st, cudaStreamNonBlocking), "stream");
+            cuda_check(cudaEventCreateWithFlags(&bt.ev, cudaEventDisableTiming), "event");
+            cuda_check(cudaMallocHost((void**)&bt.h_reqs, sizeof(MixedReq) * kMaxSlots), "pinned");
+            cuda_check(cudaMallocHost((void**)&bt.h_tiles, sizeof(int2) * s->max_tiles), "pinned");
+            cuda_check(cudaMallocHost((void**)&bt.h_ntiles, sizeof(int)), "pinned");
+            std::memset(bt.h_reqs, 0, sizeof(MixedReq) * kMaxSlots);
+            bt.d_reqs = dev_alloc(ctx, sizeof(MixedReq) * kMaxSlots);
+            bt.d_tiles = dev_alloc(ctx, sizeof(int2) * s->max_tiles);
+            bt.d_ntiles = dev_alloc(ctx, sizeof(int));
+            bt.d_counter = dev_alloc(ctx, sizeof(int));
+        }
         if (!ctx->status) {
             ctx->status = dev_alloc(ctx, sizeof(int));
             cuda_check(cudaMemset(ctx->status->p, 0, sizeof(int)), "memset");
@@ -636,23 +686,30 @@ void bsar_server_destroy(bsar_server* s)
     {
         std::lock_guard<std::mutex> lk(s->ctx->mu);
         cudaSetDevice(s->ctx->device);
-        if (s->run) cudaStreamSynchronize(s->run);
+        for (ServeBatch& bt : s->batch)
+            if (bt.st) cudaStreamSynchronize(bt.st);
         if (s->io) cudaStreamSynchronize(s->io);
-        for (auto& kv : s->graphs) cudaGraphExecDestroy(kv.second);
+        cudaStream_t saved = s->ctx->stream;
+        s->ctx->stream = s->io ? s->io : saved;     // pooled request buffers are released on `io`
         for (auto& kv : s->reqs) {
             kv.second->scene.reset();
             kv.second->axes.reset();
             kv.second->image.reset();
         }
-        s->d_reqs.reset();
-        s->d_tiles.reset();
-        s->d_ntiles.reset();
-        s->d_counter.reset();
-        if (s->h_reqs) cudaFreeHost(s->h_reqs);
-        if (s->h_tiles) cudaFreeHost(s->h_tiles);
-        if (s->h_ntiles) cudaFreeHost(s->h_ntiles);
-        if (s->ev_done) cudaEventDestroy(s->ev_done);
-        if (s->run) cudaStreamDestroy(s->run);
+        if (s->io) cudaStreamSynchronize(s->io);
+        s->ctx->stream = saved;
+        for (ServeBatch& bt : s->batch) {
+            for (auto& kv : bt.graphs) cudaGraphExecDestroy(kv.second);
+            bt.d_reqs.reset();
+            bt.d_tiles.reset();
+            bt.d_ntiles.reset();
+            bt.d_counter.reset();
+            if (bt.h_reqs) cudaFreeHost(bt.h_reqs);
+            if (bt.h_tiles) cudaFreeHost(bt.h_tiles);
+            if (bt.h_ntiles) cudaFreeHost(bt.h_ntiles);
+            if (bt.ev) cudaEventDestroy(bt.ev);
+            if (bt.st) cudaStreamDestroy(bt.st);
+        }
         if (s->io) cudaStreamDestroy(s->io);
     }
     delete s;

@@ -91,12 +91,18 @@ struct bsar_ctx {
     std::unique_ptr<DevBuf> status;
     // one-request mixed launch: request record and work counter
     std::unique_ptr<DevBuf> mixed_req, mixed_counter;
+    // stream-ordered pool: while `use_pool` is set, buffers come from it (allocation and
+    // release on the current stream, without the device-wide synchronisation of
+    // cudaMalloc / cudaFree); the server's admission path runs this way next to batches
+    cudaMemPool_t pool = nullptr;
+    bool use_pool = false;
 };
 
 struct DevBuf {
     bsar_ctx* ctx = nullptr;
     void* p = nullptr;
     size_t bytes = 0;
+    bool pooled = false;
     DevBuf() = default;
     DevBuf(bsar_ctx* c, size_t n) : ctx(c), bytes(n)
     {
@@ -104,19 +110,25 @@ struct DevBuf {
         if (ctx->used + n > ctx->budget)
             fail(BSAR_ERR_OOM_BUDGET, "request of %zu bytes exceeds the HBM budget (%llu of %llu bytes in use)", n,
                  (unsigned long long)ctx->used, (unsigned long long)ctx->budget);
-        cudaError_t e = cudaMalloc(&p, n);
+        pooled = ctx->use_pool && ctx->pool;
+        cudaError_t e = pooled ? cudaMallocFromPoolAsync(&p, n, ctx->pool, ctx->stream) : cudaMalloc(&p, n);
         if (e != cudaSuccess) {
             p = nullptr;
             cudaGetLastError();
-            fail(e == cudaErrorMemoryAllocation ? BSAR_ERR_OOM_BUDGET : BSAR_ERR_CUDA, "cudaMalloc(%zu): %s", n,
-                 cudaGetErrorString(e));
+            fail(e == cudaErrorMemoryAllocation ? BSAR_ERR_OOM_BUDGET : BSAR_ERR_CUDA, "device allocation (%zu): %s",
+                 n, cudaGetErrorString(e));
         }
         ctx->used += n;
     }
+    // A pooled buffer is released on the context's current stream: every use of it has
+    // finished (the owner synchronised, or saw the using work complete) before release.
     ~DevBuf()
     {
         if (p) {
-            cudaFree(p);
+            if (pooled)
+                cudaFreeAsync(p, ctx->stream);
+            else
+                cudaFree(p);
             ctx->used -= bytes;
         }
     }
