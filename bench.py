@@ -124,10 +124,12 @@ def sfu_ops_per_voxel_pulse(W: int) -> int:
     return 2 * per_solve + 2
 
 
-def make_workload(cfg: int, rank: int):
+def make_workload(cfg: int, rank: int, nz: int = 0):
     from bsar import scene as S
 
     spec = S.config_spec(cfg)
+    if nz:
+        spec = S.scaled(spec, nz=nz)
     sc = S.make_scene(spec)
     if rank:
         # weak scaling: rank r images the next z-slab of the same size
@@ -310,7 +312,7 @@ def run_reference(args):
 
     threads = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(threads))
-    sc = make_workload(args.config, 0)
+    sc = make_workload(args.config, 0, args.nz)
     sp = sc.spec
     rates = []
     details = None
@@ -343,6 +345,8 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=15.0, help="CPU work per reference sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the comparator forms")
+    ap.add_argument("--nz", type=int, default=0, help="z-slices of the imaging grid (0: the scene's own; a "
+                    "smaller grid of the same scene is the profiling case)")
     ap.add_argument("--serve-requests", type=int, default=512, help="requests of the served workload (0: skip)")
     ap.add_argument("--serve-burst", type=int, default=64, help="requests of the capacity burst")
     ap.add_argument("--serve-fp64-sample", type=int, default=24, help="requests run serially in FP64")
@@ -375,7 +379,7 @@ def main():
         ctx.close()
         return 0
 
-    sc = make_workload(args.config, rank)
+    sc = make_workload(args.config, rank, args.nz)
     sp = sc.spec
     stream = torch.cuda.Stream()
     ctx = bsar.Context(local)
