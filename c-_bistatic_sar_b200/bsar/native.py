@@ -129,6 +129,7 @@ def lib() -> C.CDLL:
         "bsar_scene_read_stored": ([V, C.c_uint64, _i32, _d], _i32),
         "bsar_backproject": ([V, C.c_uint64, C.POINTER(Grid), C.POINTER(BpOpts), _d], _i32),
         "bsar_backproject_device": ([V, C.c_uint64, C.POINTER(Grid), C.POINTER(BpOpts), V], _i32),
+        "bsar_backproject_mixed_noalloc": ([V, C.c_uint64, C.POINTER(Grid), C.POINTER(BpOpts), _d], _i32),
         "bsar_server_create": ([V, C.POINTER(ServerOpts), C.POINTER(V)], _i32),
         "bsar_server_submit": ([V, C.POINTER(Request), C.POINTER(C.c_uint64)], _i32),
         "bsar_server_estimate": ([C.POINTER(Request), C.POINTER(C.c_uint64)], _i32),
@@ -335,6 +336,15 @@ class Context:
         o = BpOpts(SOLVER[solver], LEGS[legs], PRECISION[precision], 0, search_radius_m)
         out = np.empty((g.nx, g.ny, g.nz), dtype=np.complex128)
         self._ok(self.L.bsar_backproject(self.h, sid, C.byref(g), C.byref(o), _p(out.view(np.float64))))
+        return out
+
+    def backproject_mixed_noalloc(self, sid: int, gx, gy, gz, *, precision="mixed", search_radius_m=0.0):
+        """Mixed back-projection without device allocations (fixed per-device scratch;
+        the scene must already be compressed for `precision`)."""
+        keep, g = self._grid(gx, gy, gz)
+        o = BpOpts(SOLVER["newton"], LEGS["per_pulse"], PRECISION[precision], 0, search_radius_m)
+        out = np.empty((g.nx, g.ny, g.nz), dtype=np.complex128)
+        self._ok(self.L.bsar_backproject_mixed_noalloc(self.h, sid, C.byref(g), C.byref(o), _p(out.view(np.float64))))
         return out
 
     def backproject_device(self, sid: int, gx, gy, gz, d_image_ptr: int, *, solver="grid", legs="mean",

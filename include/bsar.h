@@ -232,6 +232,17 @@ bsar_status bsar_backproject(bsar_ctx* ctx, bsar_scene_id scene, const bsar_grid
 bsar_status bsar_backproject_device(bsar_ctx* ctx, bsar_scene_id scene, const bsar_grid* grid,
                                     const bsar_bp_opts* opts, void* d_image);
 
+/* No counterpart in the reference.  The mixed back-projection of bsar_backproject
+ * (Newton, per-pulse legs, precision BSAR_MIXED or BSAR_MIXED_FP16) with no device
+ * allocation: request record, work counter, status word, anchors, grid axes and image
+ * live in one fixed 64 MiB scratch array per device (the call fails with
+ * BSAR_ERR_INVALID_ARG when they do not fit; about 4M voxels).  The scene must already
+ * hold samples for the precision (bsar_scene_compress).  Calls that overlap in time on
+ * one device race on the scratch.  The first call on a device sets the scratch up; make
+ * it before any stream capture. */
+bsar_status bsar_backproject_mixed_noalloc(bsar_ctx* ctx, bsar_scene_id scene, const bsar_grid* grid,
+                                           const bsar_bp_opts* opts, double* image_out);
+
 /* ---------------------------------------------------------------------------------
  * Serving: image-formation requests of different grids, pulse counts and DEMs are
  * admitted as they arrive (FIFO) against an HBM budget; each admitted request's scene

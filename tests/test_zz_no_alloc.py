@@ -1,0 +1,92 @@
+"""bsar_backproject_mixed_noalloc: the mixed back-projection with no device allocation
+(request record, counter, status, anchors, axes and image in a fixed per-device scratch
+array) against the allocating entry point bsar_backproject, on two calls in a row."""
+import numpy as np
+import pytest
+
+import bsar
+from bsar import scene as S
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def scene():
+    return S.make_scene(S.scaled(S.config_spec(2), n_pulses=40, n_samples=4096, nx=13, ny=11, nz=6, dxy=0.1,
+                                 dz=0.1, n_scatterers=4))
+
+
+def _alloc(ctx, sid, gx, gy, gz, precision):
+    return ctx.backproject(sid, gx, gy, gz, solver="newton", legs="per_pulse", precision=precision)
+
+
+@pytest.mark.parametrize("precision", ["mixed", "mixed_fp16"])
+def test_noalloc_matches_allocating_entry_point(ctx, scene, precision):
+    sid = bsar.upload_scene(ctx, scene)
+    try:
+        ctx.scene_compress(sid, precision)
+        ref = _alloc(ctx, sid, scene.gx, scene.gy, scene.gz, precision)
+        used = ctx.bytes_in_use
+        first = ctx.backproject_mixed_noalloc(sid, scene.gx, scene.gy, scene.gz, precision=precision)
+        second = ctx.backproject_mixed_noalloc(sid, scene.gx, scene.gy, scene.gz, precision=precision)
+        assert ctx.bytes_in_use == used
+    finally:
+        ctx.scene_release(sid)
+    assert np.array_equal(first, ref)
+    assert np.array_equal(second, ref)
+
+
+def test_noalloc_two_grids_in_a_row(ctx, scene):
+    """A second call on another grid reuses the scratch: counter, status and image are
+    reset, nothing of the first call leaks into the second."""
+    gx2 = scene.gx[2:9] + 0.013
+    gz2 = scene.gz[:4] - 0.05
+    sid = bsar.upload_scene(ctx, scene)
+    try:
+        ctx.scene_compress(sid, "mixed")
+        a = ctx.backproject_mixed_noalloc(sid, scene.gx, scene.gy, scene.gz)
+        b = ctx.backproject_mixed_noalloc(sid, gx2, scene.gy, gz2)
+        ra = _alloc(ctx, sid, scene.gx, scene.gy, scene.gz, "mixed")
+        rb = _alloc(ctx, sid, gx2, scene.gy, gz2, "mixed")
+    finally:
+        ctx.scene_release(sid)
+    assert np.array_equal(a, ra)
+    assert np.array_equal(b, rb)
+
+
+def test_noalloc_requires_compressed_scene(ctx, scene):
+    sid = bsar.upload_scene(ctx, scene)
+    try:
+        used = ctx.bytes_in_use
+        with pytest.raises(bsar.BsarError) as e:
+            ctx.backproject_mixed_noalloc(sid, scene.gx, scene.gy, scene.gz)
+        assert e.value.status == 1 and "bsar_scene_compress" in str(e.value)
+        assert ctx.bytes_in_use == used
+    finally:
+        ctx.scene_release(sid)
+
+
+def test_noalloc_rejects_grid_beyond_scratch(ctx, scene):
+    sid = bsar.upload_scene(ctx, scene)
+    try:
+        ctx.scene_compress(sid, "mixed")
+        gx = 20.0 + 0.01 * np.arange(200)
+        gz = -5.0 + 0.01 * np.arange(120)
+        with pytest.raises(bsar.BsarError) as e:
+            ctx.backproject_mixed_noalloc(sid, gx, gx - 20.0, gz)
+        assert e.value.status == 1 and "scratch" in str(e.value)
+    finally:
+        ctx.scene_release(sid)
+
+
+def test_noalloc_rejects_fp64(ctx, scene):
+    sid = bsar.upload_scene(ctx, scene)
+    try:
+        keep, g = ctx._grid(scene.gx, scene.gy, scene.gz)
+        out = np.empty((len(scene.gx), len(scene.gy), len(scene.gz)), dtype=np.complex128)
+        o = bsar.native.BpOpts(1, 1, 0, 0, 0.0)          # Newton, per-pulse, FP64
+        st = ctx.L.bsar_backproject_mixed_noalloc(ctx.h, sid, bsar.native.C.byref(g), bsar.native.C.byref(o),
+                                                  bsar.native._p(out.view(np.float64)))
+        assert st == 6
+    finally:
+        ctx.scene_release(sid)
