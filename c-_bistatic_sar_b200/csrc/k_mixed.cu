@@ -40,8 +40,15 @@ namespace {
 
 constexpr int TI = kMixedTileI;    // tile columns (x); 272 B rows, a multiple of 16 B
 constexpr int TJ = kMixedTileJ;    // tile rows (y)
-constexpr float kTieM = 1.0e-4f;   // metres: FP32 node-scan ranking ambiguity threshold
-constexpr float kStartBand = 2.0e-3f;  // node units: FP32 start too close to a cell boundary
+// FP32 node-scan ranking ambiguity threshold, metres of optical path.  The largest FP32
+// error of a node's ranking value measured against FP64 over 6e9 medium-scene solves was
+// 4.8e-6 m (in units of L / ng), so two nodes are mis-ordered only within ~1e-5 m.
+constexpr float kTieM = 5.0e-5f;
+// A FP32 flat start closer than this to a node-cell boundary is redone in FP64: metres
+// of start-position error (the largest measured FP32 start error was 3.1e-5 node units,
+// 7.6e-6 m) plus the FP32 quantisation of the node coordinate (ulps of the largest index).
+constexpr float kStartBandM = 2.5e-5f;
+constexpr float kStartBandUlps = 8.0f;
 constexpr long kWaitSpins = 1L << 24;
 
 struct Facet32 {
@@ -57,7 +64,28 @@ struct MixedCtx {
     float istepx, istepy;           // 1 / spacing
     double ox, oy;                  // origin of the FP32 frame (first DEM node)
     double idx64, idy64;            // 1 / spacing, FP64
+    float start_band;               // node units: FP32 starts this close to a cell boundary go FP64
 };
+
+// Start heights under a voxel (the lower endpoint of both of its paths when the ground
+// index exceeds the air index): FP32 bilinear for the FP32 start, the FP64 DEM lookup for
+// the FP64 start.  Computed once per voxel instead of once per solve.
+struct VoxelStart {
+    float h32;
+    double h64;
+};
+
+}  // namespace
+
+// Start band of a DEM (node units), see kStartBandM.
+float mixed_start_band(const DemView& d)
+{
+    const double step = d.stepx < d.stepy ? d.stepx : d.stepy;
+    const double nmax = (double)(d.nx > d.ny ? d.nx : d.ny);
+    return (float)((double)kStartBandM / step + (double)kStartBandUlps * nmax * 0x1.0p-23);
+}
+
+namespace {
 
 // A DEM tile in shared memory: node (i, j) at s[(j - j0) * TI + (i - i0)].
 struct Tile {
@@ -398,14 +426,14 @@ __device__ __noinline__ int2 rerank64(const DemView d, const MixedCtx m, const f
 // FP64 flat-interface start and its nearest node, exactly as the FP64 solver makes them
 // (used when the FP32 start lies within rounding distance of a node-cell boundary).
 __device__ __noinline__ int2 start_node64(const DemView d, double Ax, double Ay, double Az, double Bx, double By,
-                                          double Bz, double na, double nb)
+                                          double Bz, double na, double nb, double h0_known)
 {
     const double A[3] = {Ax, Ay, Az}, B[3] = {Bx, By, Bz};
     const bool lower_b = nb >= na;
     const double* Lp = lower_b ? B : A;
     const double* Up = lower_b ? A : B;
     double nl = lower_b ? nb : na, nu = lower_b ? na : nb;
-    double h0 = dem_elevation(d, Lp[0], Lp[1]);
+    const double h0 = isnan(h0_known) ? dem_elevation(d, Lp[0], Lp[1]) : h0_known;
     double sx, sy;
     flat_start(Up, Lp, nu, nl, h0, kFlatIters, sx, sy);
     return make_int2(nearest_node(d.x0, d.stepx, d.nx, sx), nearest_node(d.y0, d.stepy, d.ny, sy));
@@ -418,15 +446,16 @@ __device__ __noinline__ int2 start_node64(const DemView d, double Ax, double Ay,
 template <int WT, bool TABLE>
 __device__ __forceinline__ double solve_mixed(const DemView& d, const MixedCtx& m, const Tile& T, float* table_buf,
                                               const double A[3], const double B[3], const float A32[3],
-                                              const float B32[3], float na, float nb, bool g_is_b, int W, double& dA,
-                                              double& dB, double* X = nullptr)
+                                              const float B32[3], float na, float nb, bool g_is_b, int W,
+                                              const VoxelStart& vs, double& dA, double& dB, double* X = nullptr)
 {
-    // 1. flat-interface start (FP32)
+    // 1. flat-interface start (FP32); the lower endpoint is normally the voxel itself
     const bool lower_b = nb >= na;
+    const bool lp_is_g = lower_b == g_is_b;
     const float* Lp = lower_b ? B32 : A32;
     const float* Up = lower_b ? A32 : B32;
     const float nl = lower_b ? nb : na, nu = lower_b ? na : nb;
-    float h0 = height32(m, Lp[0], Lp[1]);
+    const float h0 = lp_is_g ? vs.h32 : height32(m, Lp[0], Lp[1]);
     float hx = Lp[0] - Up[0], hy = Lp[1] - Up[1];
     const float D2 = hx * hx + hy * hy;
     float D = D2 * rsqrtf(D2);
@@ -452,8 +481,9 @@ __device__ __forceinline__ double solve_mixed(const DemView& d, const MixedCtx& 
     const float fx = sx * m.istepx, fy = sy * m.istepy;
     int is = min(max(__float2int_rn(fx), 0), m.nx - 1);
     int js = min(max(__float2int_rn(fy), 0), m.ny - 1);
-    if (fabsf(fabsf(fx - rintf(fx)) - 0.5f) < kStartBand || fabsf(fabsf(fy - rintf(fy)) - 0.5f) < kStartBand) {
-        const int2 s64 = start_node64(d, A[0], A[1], A[2], B[0], B[1], B[2], (double)na, (double)nb);
+    if (fabsf(fabsf(fx - rintf(fx)) - 0.5f) < m.start_band || fabsf(fabsf(fy - rintf(fy)) - 0.5f) < m.start_band) {
+        const int2 s64 = start_node64(d, A[0], A[1], A[2], B[0], B[1], B[2], (double)na, (double)nb,
+                                      lp_is_g ? vs.h64 : (double)NAN);
         is = s64.x;
         js = s64.y;
     }
@@ -586,6 +616,7 @@ __device__ __forceinline__ MixedCtx req_ctx(const MixedReq& r)
     m.oy = r.oy;
     m.idx64 = r.idx64;
     m.idy64 = r.idy64;
+    m.start_band = r.start_band;
     return m;
 }
 
@@ -607,6 +638,7 @@ __device__ __forceinline__ void voxel_mixed(const BpArgs& a, const MixedCtx& m, 
     const int zi = (int)(v / ((int64_t)a.nx * a.ny));
     const double P[3] = {__ldg(a.gx + xi), __ldg(a.gy + yi), __ldg(a.gz + zi)};
     const float P32[3] = {(float)(P[0] - m.ox), (float)(P[1] - m.oy), (float)P[2]};
+    const VoxelStart vs{height32(m, P32[0], P32[1]), dem_elevation(a.dem, P[0], P[1])};
     float accr = 0.f, acci = 0.f, cmpr = 0.f, cmpi = 0.f;
     for (int i = 0; i < np; i++) {
         const double Tx[3] = {__ldg(a.tx + 3 * i), __ldg(a.tx + 3 * i + 1), __ldg(a.tx + 3 * i + 2)};
@@ -625,7 +657,7 @@ __device__ __forceinline__ void voxel_mixed(const BpArgs& a, const MixedCtx& m, 
             const float B32[3] = {leg ? R32[0] : P32[0], leg ? R32[1] : P32[1], leg ? R32[2] : P32[2]};
             double dA, dB;
             L += solve_mixed<WT, true>(a.dem, m, T, table_buf, A, B, A32, B32, leg ? n2f : n1f, leg ? n1f : n2f,
-                                       leg == 0, a.W, dA, dB);
+                                       leg == 0, a.W, vs, dA, dB);
         }
         const float dL = (float)(L - __ldg(a.ref_L + i));
         // fast-time bin: integer anchor + FP32 offset
@@ -693,7 +725,7 @@ __device__ __forceinline__ void voxel_mixed(const BpArgs& a, const MixedCtx& m, 
 // work item are the same 128 a one-request launch gives a CTA, so a voxel's arithmetic
 // (warp tables, DEM tile, sums) does not depend on what else is in the batch.
 template <int WT>
-__global__ void __launch_bounds__(128, 5) k_bp_mixed(MixedBatch b)
+__global__ void __launch_bounds__(128, 4) k_bp_mixed(MixedBatch b)
 {
     __shared__ alignas(128) float tile_s[TI * TJ];
     __shared__ alignas(16) float air_s[4][TBI * TBJ];     // one E-leg table per warp
@@ -755,6 +787,7 @@ static MixedCtx mixed_ctx(const DemView& d, int pitch)
     m.oy = d.y0;
     m.idx64 = 1.0 / d.stepx;
     m.idy64 = 1.0 / d.stepy;
+    m.start_band = mixed_start_band(d);
     return m;
 }
 
@@ -770,7 +803,8 @@ __global__ void k_refraction_mixed(DemView d, MixedCtx m, const double* __restri
         const float A32[3] = {(float)(A[0] - m.ox), (float)(A[1] - m.oy), (float)A[2]};
         const float B32[3] = {(float)(B[0] - m.ox), (float)(B[1] - m.oy), (float)B[2]};
         double dA, dB, X[3];
-        solve_mixed<0, false>(d, m, T, nullptr, A, B, A32, B32, na, nb, true, W, dA, dB, X);
+        const VoxelStart vs{height32(m, B32[0], B32[1]), dem_elevation(d, B[0], B[1])};
+        solve_mixed<0, false>(d, m, T, nullptr, A, B, A32, B32, na, nb, true, W, vs, dA, dB, X);
         out[3 * k] = X[0];
         out[3 * k + 1] = X[1];
         out[3 * k + 2] = X[2];

@@ -99,6 +99,8 @@ struct alignas(64) MixedReq {
     double ox, oy;        // origin of the FP32 frame (first DEM node)
     double idx64, idy64;  // 1 / spacing
     float off_x, off_y;   // mean crossing offset from the voxel, metres (tile centring)
+    float start_band;     // node units: FP32 flat starts this close to a cell boundary are redone in FP64
+    float pad2;
 };
 
 // A batch of the persistent mixed kernel: `ntiles` work items (request index, tile of 128
@@ -116,6 +118,7 @@ cudaError_t launch_bp_plain(const BpArgs& a, int solver, int legs, cudaStream_t 
 cudaError_t launch_refraction_mixed(const DemView& d, int pitch, const double* p1, const double* p2, int64_t n,
                                     double n1, double n2, int W, double* out, cudaStream_t st);
 cudaError_t launch_bp_mixed(const MixedBatch& b, int W, int grid, cudaStream_t st);
+float mixed_start_band(const DemView& d);
 int mixed_grid_ctas();   // persistent grid size (SMs x resident CTAs)
 cudaError_t launch_ref_ranges(const DemView& d, const double* tx, const double* rx, int np, const double* center,
                               double n1, double n2, int W, double lambda, double bin_per_m, double* ref_L,

@@ -604,6 +604,7 @@ inline MixedReq mixed_request(const Scene* s, const BpArgs& a, bool fp16)
     r.idy64 = 1.0 / s->dem.view.stepy;
     r.off_x = s->off_x;
     r.off_y = s->off_y;
+    r.start_band = mixed_start_band(s->dem.view);
     return r;
 }
 
