@@ -339,8 +339,9 @@ class Context:
         return out
 
     def backproject_mixed_noalloc(self, sid: int, gx, gy, gz, *, precision="mixed", search_radius_m=0.0):
-        """Mixed back-projection without device allocations (fixed per-device scratch;
-        the scene must already be compressed for `precision`)."""
+        """Mixed back-projection that allocates no GPU memory, for callers whose GPU memory
+        belongs to another allocator: a fixed 64 MiB per-device scratch, one call at a
+        time per device; the scene must already be compressed for `precision`."""
         keep, g = self._grid(gx, gy, gz)
         o = BpOpts(SOLVER["newton"], LEGS["per_pulse"], PRECISION[precision], 0, search_radius_m)
         out = np.empty((g.nx, g.ny, g.nz), dtype=np.complex128)

@@ -2,6 +2,12 @@
 // with every per-call device buffer carved out of one file-scope scratch array, so a call
 // makes no device allocation (no cudaMalloc / cudaFree, no pool, no library workspace).
 //
+// Who needs it: programs whose device memory is owned by another allocator -- a
+// framework's caching allocator that has reserved most of the GPU, or a client held to a
+// fixed memory limit -- where a cudaMalloc from this library fails or forces that
+// allocator to give memory back; and latency-critical loops that cannot take the
+// device-wide wait a cudaFree implies, which stalls every other stream on the GPU.
+//
 // Scratch layout (each region 256-byte aligned):
 //   request record (MixedReq, holds the DEM tensor map)
 //   work counter + status word        -- must start at zero: cleared every call
@@ -9,10 +15,12 @@
 //   grid axes
 //   image (complex128, copied to the caller's buffer at the end)
 //
-// The scratch is one per device and per process: calls that overlap in time on one
-// device (two threads, two contexts, or an earlier call's work still on another stream)
-// race on it.  The first call on a device looks the array up (cudaGetSymbolAddress with
-// that device current) and may load the module; make it before any stream capture.
+// The array is 64 MiB, and every GPU on which the library is loaded holds it until the
+// process exits.  It is one per device and per process and keeps the previous call's
+// contents: calls that overlap in time on one device (two threads, two contexts, or an
+// earlier call's work still on another stream) race on it.  The first call on a device
+// looks the array up (cudaGetSymbolAddress with that device current) and may load the
+// module; make that first call before any stream capture.
 #include <mutex>
 
 #include "runtime.hpp"

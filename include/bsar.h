@@ -234,12 +234,16 @@ bsar_status bsar_backproject_device(bsar_ctx* ctx, bsar_scene_id scene, const bs
 
 /* No counterpart in the reference.  The mixed back-projection of bsar_backproject
  * (Newton, per-pulse legs, precision BSAR_MIXED or BSAR_MIXED_FP16) with no device
- * allocation: request record, work counter, status word, anchors, grid axes and image
- * live in one fixed 64 MiB scratch array per device (the call fails with
- * BSAR_ERR_INVALID_ARG when they do not fit; about 4M voxels).  The scene must already
- * hold samples for the precision (bsar_scene_compress).  Calls that overlap in time on
- * one device race on the scratch.  The first call on a device sets the scratch up; make
- * it before any stream capture. */
+ * allocation, for callers that cannot allocate: programs whose GPU memory is owned by
+ * another allocator (a framework's caching allocator, a client held to a memory limit),
+ * where a cudaMalloc fails or makes that allocator release memory, and latency-critical
+ * loops that cannot take the device-wide wait of a cudaFree.  Request record, work
+ * counter, status word, anchors, grid axes and image live in one fixed 64 MiB scratch
+ * array per device, held from library load to process exit (a call that does not fit,
+ * beyond about 4M voxels, fails with BSAR_ERR_INVALID_ARG).  The scene must already hold
+ * samples for the precision (bsar_scene_compress).  Calls that overlap in time on one
+ * device race on the scratch.  The first call on a device sets the scratch up; make it
+ * before any stream capture. */
 bsar_status bsar_backproject_mixed_noalloc(bsar_ctx* ctx, bsar_scene_id scene, const bsar_grid* grid,
                                            const bsar_bp_opts* opts, double* image_out);
 

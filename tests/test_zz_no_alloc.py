@@ -1,6 +1,7 @@
-"""bsar_backproject_mixed_noalloc: the mixed back-projection with no device allocation
-(request record, counter, status, anchors, axes and image in a fixed per-device scratch
-array) against the allocating entry point bsar_backproject, on two calls in a row."""
+"""bsar_backproject_mixed_noalloc, the entry point for callers that cannot allocate GPU
+memory (another allocator owns it, or a cudaFree's device-wide wait is not allowed):
+its image must equal the allocating entry point bsar_backproject's, on two calls in a
+row that share the fixed per-device scratch array."""
 import numpy as np
 import pytest
 
