@@ -29,6 +29,7 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 
 #include "dev_common.cuh"
@@ -296,19 +297,20 @@ __device__ __noinline__ Rank scan_generic(const MixedCtx m, const float* ts, int
     return r;
 }
 
-// Per-warp table of the E-leg term re |N-E| over the union of the 32 lanes' windows (all
-// lanes solve the same pulse, so this leg does not depend on the voxel).  Lane l fills
-// column j0 + l.  Warp-uniform; `ok` is false when the union does not fit.
+// Per-warp table over the union of the 32 lanes' windows: (z, re |N-E|) per node, the
+// height next to the E-leg term (all lanes solve the same pulse, so this leg does not
+// depend on the voxel), so the scan reads both with one 8-byte load.  Lane l fills column
+// j0 + l.  Warp-uniform; `ok` is false when the union does not fit.
 constexpr int TBJ = 32;
-constexpr int TBI = 24;
+constexpr int TBI = 20;
 
 struct AirTable {
-    float* t;
+    float2* t;
     int i0, j0;
     bool ok;
 };
 
-__device__ __forceinline__ AirTable build_air_table(const MixedCtx& m, const Tile& T, float* buf, int is, int js, int W,
+__device__ __forceinline__ AirTable build_air_table(const MixedCtx& m, const Tile& T, float2* buf, int is, int js, int W,
                                                     float ex, float ey, float ez, float re)
 {
     const unsigned full = 0xffffffffu;
@@ -327,7 +329,7 @@ __device__ __forceinline__ AirTable build_air_table(const MixedCtx& m, const Til
             float z = in_tile ? T.s[(j - T.j0) * TI + (i - T.i0)] : zf(m, i, j);
             float dx = (float)i * m.stepx - ex, dz = z - ez;
             float q = fmaf(dz, dz, fmaf(dx, dx, sy));
-            buf[(i - i0) * TBJ + lane] = re * (q * rsqrtf(q));
+            buf[(i - i0) * TBJ + lane] = make_float2(z, re * (q * rsqrtf(q)));
         }
     }
     __syncwarp();
@@ -335,11 +337,12 @@ __device__ __forceinline__ AirTable build_air_table(const MixedCtx& m, const Til
     return A;
 }
 
-// Full (2W+1)^2 window inside the DEM, the tile and the warp table: the E leg from the
-// table, the G leg per node, columns unrolled with compile-time offsets.
+// Full (2W+1)^2 window inside the DEM and the warp table: height and E leg from the
+// table (one 8-byte load per node), the G leg per node, columns unrolled with
+// compile-time offsets.  The best node's row is updated once per row.
 template <int W>
-__device__ __forceinline__ void scan_table(const MixedCtx& m, const Tile& T, const AirTable& AT, int is, int js,
-                                           float gx, float gy, float gz, float& v1, float& v2, int& bi, int& bj)
+__device__ __forceinline__ void scan_table(const MixedCtx& m, const AirTable& AT, int is, int js, float gx, float gy,
+                                           float gz, float& v1, float& v2, int& bi, int& bj)
 {
     constexpr int NJ = 2 * W + 1;
     float syg[NJ];
@@ -348,21 +351,27 @@ __device__ __forceinline__ void scan_table(const MixedCtx& m, const Tile& T, con
         float dy = (float)(js - W + c) * m.stepy - gy;
         syg[c] = dy * dy;
     }
-    const float* zc0 = T.s + (js - W - T.j0) * TI - T.i0;
-    const float* ac0 = AT.t + (js - W - AT.j0) - AT.i0 * TBJ;
+    const float2* row0 = AT.t + (is - W - AT.i0) * TBJ + (js - W - AT.j0);
     int bc = bj - (js - W);
 #pragma unroll 1
-    for (int i = is - W; i <= is + W; i++) {
-        float dx = (float)i * m.stepx - gx;
-        float sxg = dx * dx;
-        const float* zc = zc0 + i;
-        const float* ac = ac0 + i * TBJ;
+    for (int r = 0; r < NJ; r++) {
+        const int i = is - W + r;
+        const float dx = (float)i * m.stepx - gx;
+        const float sxg = dx * dx;
+        const float2* row = row0 + r * TBJ;
+        const float v1_row = v1;
 #pragma unroll
         for (int c = 0; c < NJ; c++) {
-            float dz = zc[c * TI] - gz;
-            float q = fmaf(dz, dz, sxg + syg[c]);
-            rank(fmaf(q, rsqrtf(q), ac[c]), i, c, v1, v2, bi, bc);
+            const float2 e = row[c];
+            const float dz = e.x - gz;
+            const float q = fmaf(dz, dz, sxg + syg[c]);
+            const float L = fmaf(q, rsqrtf(q), e.y);
+            v2 = fminf(v2, fmaxf(v1, L));
+            const bool p = L < v1;
+            v1 = p ? L : v1;
+            bc = p ? c : bc;
         }
+        bi = (v1 < v1_row) ? i : bi;
     }
     bj = js - W + bc;
 }
@@ -377,7 +386,7 @@ __device__ __forceinline__ void node_scan(const MixedCtx& m, const Tile& T, cons
     const bool in_tile = T.ok && ia >= T.i0 && ib < T.i0 + TI && ja >= T.j0 && jb < T.j0 + TJ;
     if constexpr (W > 0 && TABLE) {
         if (AT.ok && in_tile && Wr == W && ia == is - W && ib == is + W && ja == js - W && jb == js + W) {
-            scan_table<W>(m, T, AT, is, js, G[0], G[1], G[2], v1, v2, bi, bj);
+            scan_table<W>(m, AT, is, js, G[0], G[1], G[2], v1, v2, bi, bj);
             return;
         }
     }
@@ -444,7 +453,7 @@ __device__ __noinline__ int2 start_node64(const DemView d, double Ax, double Ay,
 // warp builds and uses the shared E-leg table (all 32 lanes must call together).
 // Returns the FP64 optical path; dA, dB: FP64 leg lengths; X (optional): the crossing.
 template <int WT, bool TABLE>
-__device__ __forceinline__ double solve_mixed(const DemView& d, const MixedCtx& m, const Tile& T, float* table_buf,
+__device__ __forceinline__ double solve_mixed(const DemView& d, const MixedCtx& m, const Tile& T, float2* table_buf,
                                               const double A[3], const double B[3], const float A32[3],
                                               const float B32[3], float na, float nb, bool g_is_b, int W,
                                               const VoxelStart& vs, double& dA, double& dB, double* X = nullptr)
@@ -623,7 +632,7 @@ __device__ __forceinline__ MixedCtx req_ctx(const MixedReq& r)
 // One voxel of a request over all its pulses (k: index in the request's voxel range;
 // k >= v_count repeats the last voxel without storing it, so whole warps stay active).
 template <int WT>
-__device__ __forceinline__ void voxel_mixed(const BpArgs& a, const MixedCtx& m, const Tile& T, float* table_buf,
+__device__ __forceinline__ void voxel_mixed(const BpArgs& a, const MixedCtx& m, const Tile& T, float2* table_buf,
                                             bool fp16, int64_t kk)
 {
     const int np = a.np;
@@ -728,10 +737,10 @@ template <int WT>
 __global__ void __launch_bounds__(128, 4) k_bp_mixed(MixedBatch b)
 {
     __shared__ alignas(128) float tile_s[TI * TJ];
-    __shared__ alignas(16) float air_s[4][TBI * TBJ];     // one E-leg table per warp
+    __shared__ alignas(16) float2 air_s[4][TBI * TBJ];    // one (z, E-leg) table per warp
     __shared__ alignas(8) uint64_t mbar;
     __shared__ int2 work;
-    float* table_buf = air_s[threadIdx.x >> 5];
+    float2* table_buf = air_s[threadIdx.x >> 5];
     const int ntiles = b.ntiles_dev ? *b.ntiles_dev : b.ntiles;
     if (threadIdx.x == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)) : "memory");
@@ -820,8 +829,35 @@ cudaError_t launch_refraction_mixed(const DemView& d, int pitch, const double* p
     return cudaGetLastError();
 }
 
+// Shared-memory carve-out for 4 resident CTAs per SM (DEM tile + 4 warp tables each),
+// set once per device; the rest of the unified L1 stays cache for the sample gathers.
+template <int WT> static void set_carveout()
+{
+    cudaFuncAttributes fa{};
+    if (cudaFuncGetAttributes(&fa, k_bp_mixed<WT>) != cudaSuccess) return;
+    const double need = 4.0 * (double)(fa.sharedSizeBytes + 1024);
+    int pct = (int)(100.0 * need / (228.0 * 1024.0)) + 1;
+    pct = pct > 100 ? 100 : pct;
+    cudaFuncSetAttribute(k_bp_mixed<WT>, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+}
+
+static void mixed_setup_device()
+{
+    static std::atomic<uint64_t> done{0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const uint64_t bit = 1ull << (dev & 63);
+    if (done.load() & bit) return;
+    set_carveout<0>();
+    set_carveout<3>();
+    set_carveout<6>();
+    set_carveout<12>();
+    done.fetch_or(bit);
+}
+
 int mixed_grid_ctas()
 {
+    mixed_setup_device();
     static int ctas = 0;
     if (!ctas) {
         int dev = 0, sms = 148, per = 0;
@@ -835,6 +871,7 @@ int mixed_grid_ctas()
 
 cudaError_t launch_bp_mixed(const MixedBatch& b, int W, int grid, cudaStream_t st)
 {
+    mixed_setup_device();
     switch (W) {
     case 3: k_bp_mixed<3><<<grid, 128, 0, st>>>(b); break;
     case 6: k_bp_mixed<6><<<grid, 128, 0, st>>>(b); break;
