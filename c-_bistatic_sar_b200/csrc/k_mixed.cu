@@ -432,6 +432,65 @@ __device__ __noinline__ int2 rerank64(const DemView d, const MixedCtx m, const f
     return best_ij;
 }
 
+// Warp-cooperative form of rerank64: each lane whose FP32 runner-up lies within the tie
+// band (`need`) has its window re-ranked by the whole warp, 32 nodes at a time, with the
+// same FP32 filter and FP64 node values; the smallest FP64 value with the lowest i-major
+// index wins, which is the node the FP64 scan's strict < keeps.  All 32 lanes call it.
+__device__ __noinline__ int2 rerank64_warp(const DemView d, const MixedCtx m, const float* ts, int ti0, int tj0,
+                                           bool tok, bool need, int is, int js, int Wr, float ex, float ey, float ez,
+                                           float gx, float gy, float gz, float re, float limit, double Ax, double Ay,
+                                           double Az, double Bx, double By, double Bz, double na, double nb,
+                                           int2 best_ij)
+{
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    unsigned pending = __ballot_sync(full, need);
+    int2 result = best_ij;
+    while (pending) {
+        const int l = __ffs(pending) - 1;
+        pending &= pending - 1;
+        const int lis = __shfl_sync(full, is, l), ljs = __shfl_sync(full, js, l);
+        const float lex = __shfl_sync(full, ex, l), ley = __shfl_sync(full, ey, l), lez = __shfl_sync(full, ez, l);
+        const float lgx = __shfl_sync(full, gx, l), lgy = __shfl_sync(full, gy, l), lgz = __shfl_sync(full, gz, l);
+        const float llim = __shfl_sync(full, limit, l);
+        const double A[3] = {__shfl_sync(full, Ax, l), __shfl_sync(full, Ay, l), __shfl_sync(full, Az, l)};
+        const double B[3] = {__shfl_sync(full, Bx, l), __shfl_sync(full, By, l), __shfl_sync(full, Bz, l)};
+        const int ia = max(lis - Wr, 0), ib = min(lis + Wr, m.nx - 1);
+        const int ja = max(ljs - Wr, 0), jb = min(ljs + Wr, m.ny - 1);
+        const bool in_tile = tok && ia >= ti0 && ib < ti0 + TI && ja >= tj0 && jb < tj0 + TJ;
+        const int nj = jb - ja + 1, n = (ib - ia + 1) * nj;
+        double best = INFINITY;
+        int bidx = 0x7fffffff;
+        for (int k = lane; k < n; k += 32) {
+            const int i = ia + k / nj, j = ja + k % nj;
+            float xi = (float)i * m.stepx, yj = (float)j * m.stepy;
+            float dxe = xi - lex, dxg = xi - lgx;
+            float dye = yj - ley, dyg = yj - lgy;
+            float z = in_tile ? ts[(j - tj0) * TI + (i - ti0)] : zf(m, i, j);
+            float dze = z - lez, dzg = z - lgz;
+            float qe = dxe * dxe + dye * dye + dze * dze;
+            float qg = dxg * dxg + dyg * dyg + dzg * dzg;
+            if (re * sqrtf(qe) + sqrtf(qg) <= llim) {
+                double L = node_l64(d, i, j, A, B, na, nb);
+                if (L < best) {
+                    best = L;
+                    bidx = k;
+                }
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ob = __shfl_xor_sync(full, best, o);
+            const int oi = __shfl_xor_sync(full, bidx, o);
+            if (ob < best || (ob == best && oi < bidx)) {
+                best = ob;
+                bidx = oi;
+            }
+        }
+        if (lane == l && bidx != 0x7fffffff) result = make_int2(ia + bidx / nj, ja + bidx % nj);
+    }
+    return result;
+}
+
 // FP64 flat-interface start and its nearest node, exactly as the FP64 solver makes them
 // (used when the FP32 start lies within rounding distance of a node-cell boundary).
 __device__ __noinline__ int2 start_node64(const DemView d, double Ax, double Ay, double Az, double Bx, double By,
@@ -506,17 +565,29 @@ __device__ __forceinline__ double solve_mixed(const DemView& d, const MixedCtx& 
     int bi = is, bj = js;
     node_scan<WT, TABLE>(m, T, AT, is, js, W, E, G, re, v1, v2, bi, bj);
     const float tie = kTieM / ng;
-    if (!(v2 - v1 >= tie)) {
+    const bool need = !(v2 - v1 >= tie);
+    if constexpr (TABLE) {
+        if (__any_sync(0xffffffffu, need)) {
+            const int2 b = rerank64_warp(d, m, T.s, T.i0, T.j0, T.ok, need, is, js, W, E[0], E[1], E[2], G[0], G[1],
+                                         G[2], re, v1 + tie, A[0], A[1], A[2], B[0], B[1], B[2], (double)na,
+                                         (double)nb, make_int2(bi, bj));
+            bi = b.x;
+            bj = b.y;
+        }
+    } else if (need) {
         const int2 b = rerank64(d, m, T.s, T.i0, T.j0, T.ok, is, js, W, E[0], E[1], E[2], G[0], G[1], G[2], re,
                                 v1 + tie, A[0], A[1], A[2], B[0], B[1], B[2], (double)na, (double)nb,
                                 make_int2(bi, bj));
         bi = b.x;
         bj = b.y;
     }
-    // 3. polish the facets around the best node (FP32)
+    // 3. polish the facets around the best node (FP32); heights from the DEM tile when the
+    //    node's 3 x 3 neighbourhood lies in it
+    const bool nt = T.ok && bi - 1 >= T.i0 && bi + 1 < T.i0 + TI && bj - 1 >= T.j0 && bj + 1 < T.j0 + TJ;
+    auto zt = [&](int i, int j) { return nt ? T.s[(j - T.j0) * TI + (i - T.i0)] : zf(m, i, j); };
     float Lnode;
     {
-        float xn = (float)bi * m.stepx, yn = (float)bj * m.stepy, zn = zf(m, bi, bj);
+        float xn = (float)bi * m.stepx, yn = (float)bj * m.stepy, zn = zt(bi, bj);
         float r1x = xn - A32[0], r1y = yn - A32[1], r1z = zn - A32[2];
         float r2x = xn - B32[0], r2y = yn - B32[1], r2z = zn - B32[2];
         float q1 = r1x * r1x + r1y * r1y + r1z * r1z, q2 = r2x * r2x + r2y * r2y + r2z * r2z;
@@ -535,7 +606,7 @@ __device__ __forceinline__ double solve_mixed(const DemView& d, const MixedCtx& 
         F.dy = m.stepy;
         F.idx = m.istepx;
         F.idy = m.istepy;
-        float z00 = zf(m, fi, fj), z01 = zf(m, fi + 1, fj), z10 = zf(m, fi, fj + 1), z11 = zf(m, fi + 1, fj + 1);
+        float z00 = zt(fi, fj), z01 = zt(fi + 1, fj), z10 = zt(fi, fj + 1), z11 = zt(fi + 1, fj + 1);
         F.z00 = z00;
         F.b = z01 - z00;
         F.c = z10 - z00;
