@@ -130,7 +130,8 @@ def make_workload(cfg: int, rank: int, nz: int = 0):
     spec = S.config_spec(cfg)
     if nz:
         spec = S.scaled(spec, nz=nz)
-    sc = S.make_scene(spec)
+    # the large scene's echoes are synthesised on the GPU (bsar_scene_synthesize)
+    sc = S.make_scene(spec, with_raw=spec.n_pulses * spec.n_samples <= (1 << 24))
     if rank:
         # weak scaling: rank r images the next z-slab of the same size
         sc.gz = sc.gz - rank * spec.nz * spec.dz
@@ -148,6 +149,8 @@ def time_device(ctx, torch, stream, sid, sc, precision, solver, legs, steps, war
     ptr = img.data_ptr()
 
     def step(ev=None):
+        if ev is not None:
+            ev[2].record(stream)
         ctx.scene_compress(sid, precision)
         if ev is not None:
             ev[0].record(stream)
@@ -158,7 +161,7 @@ def time_device(ctx, torch, stream, sid, sc, precision, solver, legs, steps, war
     for _ in range(warmup):
         step()
     torch.cuda.synchronize()
-    kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    kev = [tuple(torch.cuda.Event(enable_timing=True) for _ in range(3)) for _ in range(steps)]
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
     launches0 = ctx.launches
@@ -168,13 +171,15 @@ def time_device(ctx, torch, stream, sid, sc, precision, solver, legs, steps, war
     t1.record(stream)
     torch.cuda.synchronize()
     total_ms = t0.elapsed_time(t1)
-    bp_ms = [a.elapsed_time(b) for a, b in kev]
+    bp_ms = [a.elapsed_time(b) for a, b, _ in kev]
+    time_device.pc_ms = [c.elapsed_time(a) for a, b, c in kev]
     return total_ms, bp_ms, img, ctx.launches - launches0
 
 
-def cpu_reference_rate(sc, seconds: float, threads: int, use_ref: bool = True):
-    """Reference CPU path (grid search, mean legs) on a bounded voxel sample.
-    Returns (voxel-pulses/s for a full image, details)."""
+def cpu_reference_rate(sc, seconds: float, threads: int, use_ref: bool = True, z_slices=None):
+    """Reference CPU path (grid search, mean legs) on a bounded voxel sample (uniform over
+    the grid, or over the z-slices `z_slices`).  Returns (voxel-pulses/s for a full image,
+    details incl. the sampled voxels and their values)."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as O
 
@@ -197,11 +202,21 @@ def cpu_reference_rate(sc, seconds: float, threads: int, use_ref: bool = True):
     else:
         kw["solver"] = "grid"
 
+    def pick(n):
+        if z_slices is None:
+            return rng.choice(nv_total, size=n, replace=False)
+        plane = sp.nx * sp.ny
+        zi = rng.choice(np.asarray(z_slices), size=n)
+        return zi * plane + rng.choice(plane, size=n, replace=True)
+
+    last = {}
+
     def run(n):
-        vox = rng.choice(nv_total, size=n, replace=False)
+        vox = pick(n)
         t0 = time.perf_counter()
-        impl.backproject(dem, sc.tx, sc.rx, rc, sc.gx, sc.gy, sc.gz, sp.n1, sp.n2, 3e8, sc.fs_eff, sc.lam,
-                         voxels=vox, **kw)
+        vals = impl.backproject(dem, sc.tx, sc.rx, rc, sc.gx, sc.gy, sc.gz, sp.n1, sp.n2, 3e8, sc.fs_eff, sc.lam,
+                                voxels=vox, **kw)
+        last["vox"], last["vals"] = vox, vals
         return time.perf_counter() - t0
 
     n0 = max(threads, 1)
@@ -215,7 +230,8 @@ def cpu_reference_rate(sc, seconds: float, threads: int, use_ref: bool = True):
         f"{n1} random voxels of the {sp.nx}x{sp.ny}x{sp.nz} grid x {sp.n_pulses} pulses (grid-search Fermat, "
         f"mean legs, as shipped) in {dt1:.1f} s + full pulse compression {t_pc:.1f} s and upsampling "
         f"{t_up:.1f} s; rate = full-image voxel-pulses / (compression + upsampling + per-voxel time x "
-        f"{nv_total} voxels)"), "per_voxel_s": per_voxel, "pc_s": t_pc, "upsample_s": t_up}
+        f"{nv_total} voxels)"), "per_voxel_s": per_voxel, "pc_s": t_pc, "upsample_s": t_up, "voxels": last["vox"],
+        "values": last["vals"]}
 
 
 def serve_leg(ctx, torch, n_requests: int, burst: int, fp64_sample: int, load: float = 0.8):
@@ -313,6 +329,8 @@ def run_reference(args):
     threads = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(threads))
     sc = make_workload(args.config, 0, args.nz)
+    if sc.raw is None:                     # no GPU on this arm: numpy echo synthesis
+        sc = S.make_scene(sc.spec)
     sp = sc.spec
     rates = []
     details = None
@@ -342,7 +360,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="bsar", choices=["bsar", "reference"])
     ap.add_argument("--config", type=int, default=2)
-    ap.add_argument("--ref-seconds", type=float, default=15.0, help="CPU work per reference sample")
+    ap.add_argument("--ref-seconds", type=float, default=10.0, help="CPU work per reference sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the comparator forms")
     ap.add_argument("--nz", type=int, default=0, help="z-slices of the imaging grid (0: the scene's own; a "
@@ -384,6 +402,10 @@ def main():
     stream = torch.cuda.Stream()
     ctx = bsar.Context(local)
     ctx.set_stream(stream.cuda_stream)
+    if sc.raw is None:
+        s0 = bsar.synthesize_scene(ctx, sc)
+        sc.raw = ctx.scene_read_samples(s0, sp.n_pulses, sp.n_samples)
+        ctx.scene_release(s0)
     sid = bsar.upload_scene(ctx, sc)
     W = bsar.scene.search_nodes_for(sc.x_vec, sc.y_vec)
     nv = sp.n_voxels
@@ -427,8 +449,9 @@ def main():
         ctx.scene_release(s)
         return out
 
-    e2e_steps = max(2, min(args.steps, 3))
-    e2e_step()
+    e2e_steps = max(1, min(args.steps, 3))
+    if args.warmup > 0:
+        e2e_step()
     torch.cuda.synchronize()
     barrier()
     t = time.perf_counter()
@@ -454,7 +477,8 @@ def main():
                                "ms_per_step": max_over_ranks(t16 / fs)}
         # the reference's own algorithm (grid search + mean legs, FP64) on every 20th z-slice
         gz_sub = sc.gz[::20]
-        tg, _, _, _ = time_device(ctx, torch, stream, sid, sc, "fp64", "grid", "mean", 1, 1, gz=gz_sub)
+        tg, _, img_grid, _ = time_device(ctx, torch, stream, sid, sc, "fp64", "grid", "mean", 1, 1, gz=gz_sub)
+        img_grid = img_grid.cpu().numpy().view(np.complex128).reshape(sp.nx, sp.ny, len(gz_sub))
         nv_sub = sp.nx * sp.ny * len(gz_sub)
         forms["fp64_grid_mean_reference_algorithm"] = {
             "value": world * nv_sub * sp.n_pulses / (max_over_ranks(tg) / 1e3), "ms_per_step": max_over_ranks(tg),
@@ -472,6 +496,20 @@ def main():
 
         acc = {"mixed_vs_fp64": stats(a), "mixed_fp16_vs_fp64": stats(c16),
                "e2e_image_equals_device_image": bool(np.array_equal(img_host, a))}
+        # Fermat crossing points of the mixed solver against FP64 on random (pulse, voxel) pairs
+        rng = np.random.default_rng(0x5A4B0D)
+        pi = rng.integers(0, sp.n_pulses, 1 << 16)
+        vi = rng.integers(0, [sp.nx, sp.ny, sp.nz], size=(1 << 16, 3))
+        P = np.stack([sc.gx[vi[:, 0]], sc.gy[vi[:, 1]], sc.gz[vi[:, 2]]], axis=1)
+        demA = bsar.DemArrays(sc.x_vec, sc.y_vec, sc.z)
+        cross = 0.0
+        for ant, na, nb, first in ((sc.tx, sp.n1, sp.n2, True), (sc.rx, sp.n2, sp.n1, False)):
+            p1, p2 = (ant[pi], P) if first else (P, ant[pi])
+            x64 = ctx.refraction_points(demA, p1, p2, na, nb, solver="newton")
+            x32 = ctx.refraction_points(demA, p1, p2, na, nb, solver="newton", precision="mixed")
+            cross = max(cross, float(np.linalg.norm(x32 - x64, axis=1).max()))
+        acc["mixed_fermat_crossing_max_err_m"] = cross
+        acc["fermat_sample"] = "65536 random (pulse, voxel) pairs per leg, Tx->voxel and voxel->Rx"
 
     # ---------------- roofline of the dominant kernel (k_bp_mixed) ------------------
     peaks, peak_src = _peaks()
@@ -492,11 +530,38 @@ def main():
                            "hbm_peak_gbs": peaks.get("hbm_gbs"), "peak_source": peak_src},
                 "fp32_flops_per_voxel_pulse": fp32_flops_per_voxel_pulse(W), "node_scan_half_width": W}
 
+    # pulse compression (K1): HBM roofline on raw in + upsampled complex64 out
+    pc_ms = max_over_ranks(statistics.mean(time_device.pc_ms))
+    ns = sp.n_samples
+    pc_bytes = sp.n_pulses * (16 * ns + 8 * ns * sp.upsample)
+    pc_gbs = pc_bytes / (pc_ms / 1e3) / 1e9
+    roofline["pulse_compression"] = {
+        "kernel": "k_pulse_compress<float>", "ms": pc_ms, "samples_per_s": sp.n_pulses * ns / (pc_ms / 1e3),
+        "bytes": pc_bytes, "achieved_gbs": pc_gbs, "peak_gbs": peaks.get("hbm_gbs"), "frac": pc_gbs / peaks.get("hbm_gbs", 1),
+        "flops": sp.n_pulses * 2 * (10 * ns * math.log2(ns) + 6 * ns)}
+    roofline["fermat"] = {"solves_per_s": 2 * vp / (bp_avg_ms / 1e3),
+                          "note": "two mixed Fermat solves per voxel-pulse inside k_bp_mixed"}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        rate, det = cpu_reference_rate(sc, args.ref_seconds, threads)
+        zs = list(range(0, sp.nz, 20)) if forms else None
+        rate, det = cpu_reference_rate(sc, args.ref_seconds, threads, z_slices=zs)
         cpu = {"value": rate, "unit": UNIT, "cores": det["cores"], "kind": det["kind"], "sample": det["sample"]}
+        if zs is not None:
+            v = det["voxels"]
+            plane = sp.nx * sp.ny
+            zi, xi, yi = v // plane, (v % plane) // sp.ny, v % sp.ny
+            g = img_grid[xi, yi, zi // 20]
+            ref = det["values"]
+            cpu["check_vs_gpu_fp64_grid"] = {
+                "voxels": int(len(v)), "rel_l2": float(np.linalg.norm(g - ref) / np.linalg.norm(ref)),
+                "max_abs": float(np.abs(g - ref).max())}
+        shipped = min(12, threads)
+        if shipped != threads:
+            r12, d12 = cpu_reference_rate(sc, args.ref_seconds, shipped)
+            cpu["as_shipped"] = {"value": r12, "cores": shipped,
+                                 "note": "the reference caps its OpenMP loop at 12 threads"}
 
     serving = None
     if rank == 0 and world == 1 and args.serve_requests > 0:

@@ -302,7 +302,9 @@ __device__ __noinline__ Rank scan_generic(const MixedCtx m, const float* ts, int
 // depend on the voxel), so the scan reads both with one 8-byte load.  Lane l fills column
 // j0 + l.  Warp-uniform; `ok` is false when the union does not fit.
 constexpr int TBJ = 32;
-constexpr int TBI = 20;
+// table rows for a compile-time node-scan half width: the window plus slack for the
+// spread of the 32 lanes' window centres
+template <int WT> struct TableRows { static constexpr int v = WT > 0 ? 2 * WT + 1 + (WT >= 12 ? 5 : 7) : 1; };
 
 struct AirTable {
     float2* t;
@@ -310,6 +312,7 @@ struct AirTable {
     bool ok;
 };
 
+template <int TBI>
 __device__ __forceinline__ AirTable build_air_table(const MixedCtx& m, const Tile& T, float2* buf, int is, int js, int W,
                                                     float ex, float ey, float ez, float re)
 {
@@ -385,7 +388,7 @@ __device__ __forceinline__ void node_scan(const MixedCtx& m, const Tile& T, cons
     const int ja = max(js - Wr, 0), jb = min(js + Wr, m.ny - 1);
     const bool in_tile = T.ok && ia >= T.i0 && ib < T.i0 + TI && ja >= T.j0 && jb < T.j0 + TJ;
     if constexpr (W > 0 && TABLE) {
-        if (AT.ok && in_tile && Wr == W && ia == is - W && ib == is + W && ja == js - W && jb == js + W) {
+        if (AT.ok && Wr == W && ia == is - W && ib == is + W && ja == js - W && jb == js + W) {
             scan_table<W>(m, AT, is, js, G[0], G[1], G[2], v1, v2, bi, bj);
             return;
         }
@@ -560,7 +563,8 @@ __device__ __forceinline__ double solve_mixed(const DemView& d, const MixedCtx& 
     const float ng = g_is_b ? nb : na;
     const float re = (g_is_b ? na : nb) / ng;
     AirTable AT{table_buf, 0, 0, false};
-    if constexpr (TABLE) AT = build_air_table(m, T, table_buf, is, js, W, E[0], E[1], E[2], re);
+    if constexpr (TABLE && WT > 0)
+        AT = build_air_table<TableRows<WT>::v>(m, T, table_buf, is, js, W, E[0], E[1], E[2], re);
     float v1 = INFINITY, v2 = INFINITY;
     int bi = is, bj = js;
     node_scan<WT, TABLE>(m, T, AT, is, js, W, E, G, re, v1, v2, bi, bj);
@@ -808,7 +812,7 @@ template <int WT>
 __global__ void __launch_bounds__(128, 4) k_bp_mixed(MixedBatch b)
 {
     __shared__ alignas(128) float tile_s[TI * TJ];
-    __shared__ alignas(16) float2 air_s[4][TBI * TBJ];    // one (z, E-leg) table per warp
+    __shared__ alignas(16) float2 air_s[4][TableRows<WT>::v * TBJ];   // one (z, E-leg) table per warp
     __shared__ alignas(8) uint64_t mbar;
     __shared__ int2 work;
     float2* table_buf = air_s[threadIdx.x >> 5];

@@ -36,6 +36,13 @@ def rough():
                            n_scatterers=4))
 
 
+@pytest.fixture(scope="module")
+def large():
+    # config-5 DEM and signal (1024^2 fBm at 0.125 m, so a 25 x 25 node scan; 16384
+    # samples), a 10 x 40 x 4 grid so warps span y
+    return _setup(S.scaled(S.config_spec(5), n_pulses=48, nx=10, ny=40, nz=4, n_scatterers=6))
+
+
 def _oracle_image(oracle, sc, legs, solver):
     sp = sc.spec
     dem = O.Dem(sc.x_vec, sc.y_vec, sc.z)
@@ -57,7 +64,7 @@ def test_plain_grid_matches_reference_algorithm(ctx, oracle, small, legs):
     assert np.argmax(np.abs(img)) == np.argmax(np.abs(ref))
 
 
-@pytest.mark.parametrize("which", ["small", "rough"])
+@pytest.mark.parametrize("which", ["small", "rough", "large"])
 def test_plain_newton_matches_oracle(ctx, oracle, which, request):
     sc = request.getfixturevalue(which)
     sid = bsar.upload_scene(ctx, sc)
@@ -71,7 +78,7 @@ def test_plain_newton_matches_oracle(ctx, oracle, which, request):
 
 
 @pytest.mark.parametrize("precision", ["mixed", "mixed_fp16"])
-@pytest.mark.parametrize("which", ["small", "rough"])
+@pytest.mark.parametrize("which", ["small", "rough", "large"])
 def test_mixed_matches_fp64(ctx, which, precision, request):
     sc = request.getfixturevalue(which)
     sid = bsar.upload_scene(ctx, sc)
