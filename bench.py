@@ -48,6 +48,9 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT / "c-_bistatic_sar_b200"))
 
 METRIC = "BP voxel-pulses/s (Fermat incl.), mixed vs FP64 @<=1e-3 rel-L2; served p99 ms"
+# DRAM bytes (read + write) of one k_bp_mixed launch on the full medium scene, from an ncu
+# capture of dram__bytes_read.sum + dram__bytes_write.sum (one pass) of this command
+TRAFFIC_BYTES = {2: 9.48e6}
 UNIT = "voxel-pulses/s"
 
 
@@ -521,7 +524,8 @@ def main():
     sfu_rate = sfu_ops_per_voxel_pulse(W) * vp / (bp_avg_ms / 1e3)
     sfu_peak = 148 * 16 * sm_mhz * 1e6
     roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
-                "frac": achieved / fp32_peak, "traffic": None,
+                "frac": achieved / fp32_peak,
+                "traffic": TRAFFIC_BYTES.get(args.config) if not args.nz else None,
                 "kernel": "k_bp_mixed", "kernel_ms": bp_avg_ms,
                 "peak_source": f"nominal 148 SM x 128 FP32 lanes x 2 flop x {sm_mhz:.0f} MHz (no FP32-pipe "
                                f"figure in MEASURED_PEAKS.json)",
