@@ -27,6 +27,7 @@ STATUS = {0: "ok", 1: "invalid argument", 2: "HBM budget exceeded", 3: "device w
 SOLVER = {"grid": 0, "newton": 1}
 LEGS = {"mean": 0, "per_pulse": 1}
 PRECISION = {"fp64": 0, "mixed": 1, "mixed_fp16": 2}
+FILE_LAYOUT = {"as_imager": 0, "row_major": 1}
 
 
 class BsarError(RuntimeError):
@@ -62,6 +63,11 @@ class BpOpts(C.Structure):
 
 class Opts(C.Structure):
     _fields_ = [("device", _i32), ("flags", _i32), ("hbm_budget_bytes", C.c_uint64)]
+
+
+class MatrixHeader(C.Structure):
+    _fields_ = [("ndims", C.c_uint32), ("is_complex", C.c_uint32), ("dtype_len", C.c_uint32),
+                ("dtype", C.c_char * 17), ("dims", C.c_uint64 * 8), ("total", C.c_uint64)]
 
 
 class ServerOpts(C.Structure):
@@ -130,6 +136,13 @@ def lib() -> C.CDLL:
         "bsar_backproject": ([V, C.c_uint64, C.POINTER(Grid), C.POINTER(BpOpts), _d], _i32),
         "bsar_backproject_device": ([V, C.c_uint64, C.POINTER(Grid), C.POINTER(BpOpts), V], _i32),
         "bsar_backproject_mixed_noalloc": ([V, C.c_uint64, C.POINTER(Grid), C.POINTER(BpOpts), _d], _i32),
+        "bsar_matrix_read_header": ([C.c_char_p, C.POINTER(MatrixHeader)], _i32),
+        "bsar_matrix_read": ([C.c_char_p, _d, C.c_uint64], _i32),
+        "bsar_matrix_write": ([C.c_char_p, C.c_uint32, C.POINTER(C.c_uint64), _i32, _d], _i32),
+        "bsar_scene_upload_file": ([V, C.POINTER(SceneDesc), C.c_char_p, _i32, C.POINTER(C.c_uint64)], _i32),
+        "bsar_image_export": ([C.c_char_p, _d, _i64, _i64, _i64, _d, _d, _d], _i32),
+        "bsar_image_export_device": ([V, C.c_char_p, V, _i64, _i64, _i64, _d, _d, _d], _i32),
+        "bsar_dem_load_esri": ([C.c_char_p, C.POINTER(_i64), C.POINTER(_i64), _d, _d, _d, C.POINTER(_i32)], _i32),
         "bsar_server_create": ([V, C.POINTER(ServerOpts), C.POINTER(V)], _i32),
         "bsar_server_submit": ([V, C.POINTER(Request), C.POINTER(C.c_uint64)], _i32),
         "bsar_server_estimate": ([C.POINTER(Request), C.POINTER(C.c_uint64)], _i32),
@@ -302,6 +315,25 @@ class Context:
         self._ok(self.L.bsar_scene_synthesize(self.h, C.byref(desc), _p(pos), _p(amp), len(amp), snr_db,
                                               seed & (2**64 - 1), C.byref(sid)))
         return int(sid.value)
+
+    def scene_upload_file(self, dem: DemArrays, tx, rx, path, *, layout="as_imager", kind="compressed", upsample=4,
+                          n1=1.0, n2=2.0, c=3e8, fc=1e9, fs=1.2e9, chirp_f0=0.0, chirp_f1=0.0, chirp_T=0.0) -> int:
+        """Resident scene whose pulses come from a matrix file (bsar_scene_upload_file):
+        layout "as_imager" (the imager's reading) or "row_major" (transposed on the GPU)."""
+        tx = _f64(tx, (-1, 3))
+        rx = _f64(rx, (-1, 3))
+        desc = SceneDesc(dem.c, len(tx), _p(tx), _p(rx), 0, None, 0 if kind == "raw" else 1, upsample, n1, n2, c, fc,
+                         fs, chirp_f0, chirp_f1, chirp_T)
+        sid = C.c_uint64()
+        self._ok(self.L.bsar_scene_upload_file(self.h, C.byref(desc), str(path).encode(), FILE_LAYOUT[layout],
+                                               C.byref(sid)))
+        return int(sid.value)
+
+    def image_export_device(self, path, d_image_ptr: int, nx: int, ny: int, nz: int, gx=None, gy=None, gz=None):
+        """Write a device image ([x][y][z] complex128) in the reference's file order."""
+        ax = [None if a is None else _f64(a) for a in (gx, gy, gz)]
+        self._ok(self.L.bsar_image_export_device(self.h, str(path).encode(), C.c_void_p(d_image_ptr), nx, ny, nz,
+                                                 *[_p(a) for a in ax]))
 
     def scene_read_samples(self, sid: int, n_pulses: int, n_samples: int):
         out = np.empty((n_pulses, n_samples), dtype=np.complex128)
@@ -502,3 +534,55 @@ def submit_scene(server: Server, scene, gx, gy, gz, *, synthesize=True, precisio
                              scat_amp=scene.scat_amp, snr_db=sp.snr_db if snr_db is None else snr_db,
                              seed=sp.seed if seed is None else seed, **common)
     return server.submit(dem, scene.tx, scene.rx, gx, gy, gz, samples=scene.raw, **common)
+
+
+# ---- files (no context needed) --------------------------------------------------------
+def matrix_read(path):
+    """readBinary of a matrix file: (complex128 values, dims, is_complex)."""
+    L = lib()
+    h = MatrixHeader()
+    st = L.bsar_matrix_read_header(str(path).encode(), C.byref(h))
+    if st != 0:
+        raise BsarError(st, f"cannot read the header of {path}")
+    out = np.empty(max(int(h.total), 1), dtype=np.complex128)
+    st = L.bsar_matrix_read(str(path).encode(), _p(out.view(np.float64)), int(h.total))
+    if st != 0:
+        raise BsarError(st, f"cannot read {path}")
+    return out[: int(h.total)], [int(h.dims[k]) for k in range(h.ndims)], bool(h.is_complex)
+
+
+def matrix_write(path, data):
+    """exportComplexMatrix-style file of a complex (or real) array of any rank."""
+    a = np.asarray(data)
+    cplx = np.iscomplexobj(a)
+    a = np.ascontiguousarray(a, dtype=np.complex128 if cplx else np.float64)
+    dims = (C.c_uint64 * max(a.ndim, 1))(*a.shape)
+    st = lib().bsar_matrix_write(str(path).encode(), a.ndim, dims, 1 if cplx else 0, _p(a.view(np.float64)))
+    if st != 0:
+        raise BsarError(st, f"cannot write {path}")
+
+
+def image_export(path, image, gx=None, gy=None, gz=None):
+    """export3DComplexMatrix of an [x][y][z] complex image (x fastest in the file)."""
+    img = _c128(image)
+    nx, ny, nz = img.shape
+    ax = [None if a is None else _f64(a) for a in (gx, gy, gz)]
+    st = lib().bsar_image_export(str(path).encode(), _p(img.view(np.float64)), nx, ny, nz, *[_p(a) for a in ax])
+    if st != 0:
+        raise BsarError(st, f"cannot write {path}")
+
+
+def dem_load_esri(path):
+    """loadDEM of an ESRI ASCII grid: (x_vec, y_vec, z[ny, nx], flags)."""
+    L = lib()
+    nx, ny, fl = _i64(), _i64(), _i32()
+    st = L.bsar_dem_load_esri(str(path).encode(), C.byref(nx), C.byref(ny), None, None, None, C.byref(fl))
+    if st != 0:
+        raise BsarError(st, f"cannot load {path}")
+    x = np.empty(max(nx.value, 1))
+    y = np.empty(max(ny.value, 1))
+    z = np.empty(max(nx.value * ny.value, 1))
+    st = L.bsar_dem_load_esri(str(path).encode(), C.byref(nx), C.byref(ny), _p(x), _p(y), _p(z), C.byref(fl))
+    if st != 0:
+        raise BsarError(st, f"cannot load {path}")
+    return x[: nx.value], y[: ny.value], z[: nx.value * ny.value].reshape(ny.value, nx.value), int(fl.value)

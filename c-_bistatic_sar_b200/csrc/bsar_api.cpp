@@ -9,24 +9,6 @@
 // ------------------------------------------------------------------------------------
 // API glue
 // ------------------------------------------------------------------------------------
-template <typename F> static bsar_status guarded(bsar_ctx* ctx, F&& f)
-{
-    if (!ctx) return BSAR_ERR_INVALID_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mu);
-    try {
-        cuda_check(cudaSetDevice(ctx->device), "cudaSetDevice");
-        f();
-        ctx->last_error.clear();
-        return BSAR_OK;
-    } catch (const Error& e) {
-        ctx->last_error = e.msg;
-        return e.status;
-    } catch (const std::bad_alloc&) {
-        ctx->last_error = "host allocation failed";
-        return BSAR_ERR_OOM_BUDGET;
-    }
-}
-
 extern "C" {
 
 const char* bsar_status_string(bsar_status s)

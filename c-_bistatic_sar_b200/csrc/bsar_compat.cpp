@@ -7,7 +7,9 @@
 
 #include <cmath>
 #include <fstream>
+#include <iomanip>
 #include <iostream>
+#include <type_traits>
 #include <memory>
 #include <mutex>
 #include <sstream>
@@ -50,6 +52,12 @@ void check(bsar_status s)
     std::string msg = std::string("bsar: ") + bsar_status_string(s) + ": " + bsar_last_error(context());
     if (s == BSAR_ERR_INVALID_ARG) throw std::invalid_argument(msg);
     throw std::runtime_error(msg);
+}
+
+// Host-only entry points (no context): a failure names the file.
+void check_files(bsar_status s, const std::string& path)
+{
+    if (s != BSAR_OK) throw std::runtime_error(std::string("bsar: ") + bsar_status_string(s) + ": " + path);
 }
 
 // ProcessedDEM -> packed heights (entries missing from a ragged Z_DEM read 0.0, as the
@@ -357,6 +365,142 @@ size_t FFTProcessor::nextPowerOfTwo(size_t n)
 }
 
 // ------------------------------ batched imager --------------------------------------
+
+// ---------------------------------------------------------------------------------
+// Files: readBinary / export* / loadDEM over the library's file entry points (host code;
+// no device needed).
+// ---------------------------------------------------------------------------------
+template <typename T> std::vector<std::complex<T>> readBinary(const std::string& filename, MatrixInfo& info)
+{
+    bsar_matrix_header h{};
+    bsar_status st = bsar_matrix_read_header(filename.c_str(), &h);
+    if (st == BSAR_ERR_NOT_FOUND) throw std::runtime_error("bsar: cannot open file " + filename);
+    if (st != BSAR_OK) throw std::runtime_error("bsar: cannot read the header of " + filename);
+    std::vector<std::complex<double>> v(h.total);
+    if (h.total && bsar_matrix_read(filename.c_str(), reinterpret_cast<double*>(v.data()), h.total) != BSAR_OK)
+        throw std::runtime_error("bsar: cannot read all values of " + filename);
+    info.dimensions.assign(h.dims, h.dims + h.ndims);
+    info.isComplex = h.is_complex != 0;
+    info.dataType = std::string(h.dtype, h.dtype_len);
+    info.totalElements = (size_t)h.total;
+    if constexpr (std::is_same<T, double>::value) {
+        return v;
+    } else {
+        std::vector<std::complex<T>> o(v.size());
+        for (size_t k = 0; k < v.size(); k++) o[k] = std::complex<T>((T)v[k].real(), (T)v[k].imag());
+        return o;
+    }
+}
+template std::vector<std::complex<double>> readBinary<double>(const std::string&, MatrixInfo&);
+
+template <typename T> std::vector<T> readRealBinary(const std::string& filename, MatrixInfo& info)
+{
+    auto c = readBinary<T>(filename, info);
+    std::vector<T> r(c.size());
+    for (size_t k = 0; k < c.size(); k++) r[k] = c[k].real();
+    return r;
+}
+template std::vector<double> readRealBinary<double>(const std::string&, MatrixInfo&);
+
+void exportComplexMatrix(const std::string& filename, const std::vector<std::vector<std::complex<double>>>& data)
+{
+    if (data.empty() || data[0].empty()) {
+        std::cerr << "Error: Empty data matrix" << std::endl;
+        return;
+    }
+    // rows x cols(first row), then every row as given (ragged rows as the reference writes them)
+    std::vector<std::complex<double>> flat;
+    for (const auto& row : data) flat.insert(flat.end(), row.begin(), row.end());
+    const uint64_t dims[2] = {data.size(), data[0].size()};
+    if (flat.size() == dims[0] * dims[1]) {
+        if (bsar_matrix_write(filename.c_str(), 2, dims, 1, reinterpret_cast<const double*>(flat.data())) != BSAR_OK)
+            std::cerr << "Error: Could not open file " << filename << std::endl;
+        return;
+    }
+    std::ofstream f(filename, std::ios::binary);
+    if (!f.is_open()) {
+        std::cerr << "Error: Could not open file " << filename << std::endl;
+        return;
+    }
+    const uint32_t nd = 2, cplx = 1, tlen = 6;
+    char name[16] = {'d', 'o', 'u', 'b', 'l', 'e'};
+    f.write(reinterpret_cast<const char*>(&nd), 4);
+    f.write(reinterpret_cast<const char*>(&cplx), 4);
+    f.write(reinterpret_cast<const char*>(&tlen), 4);
+    f.write(name, 16);
+    f.write(reinterpret_cast<const char*>(dims), 16);
+    f.write(reinterpret_cast<const char*>(flat.data()), 16 * flat.size());
+}
+
+void exportRealMatrix(const std::string& filename, const std::vector<std::vector<double>>& data)
+{
+    std::ofstream f(filename);
+    if (!f.is_open()) {
+        std::cerr << "Error: Could not open file " << filename << std::endl;
+        return;
+    }
+    f << std::fixed << std::setprecision(6);
+    for (const auto& row : data) {
+        for (size_t j = 0; j < row.size(); j++) {
+            if (j) f << ",";
+            f << row[j];
+        }
+        f << std::endl;
+    }
+}
+
+void exportVector(const std::string& filename, const std::vector<double>& data)
+{
+    std::ofstream f(filename);
+    if (!f.is_open()) {
+        std::cerr << "Error: Could not open file " << filename << std::endl;
+        return;
+    }
+    f << std::fixed << std::setprecision(6);
+    for (size_t i = 0; i < data.size(); i++) {
+        if (i) f << ",";
+        f << data[i];
+    }
+    f << std::endl;
+}
+
+void export3DComplexMatrix(const std::string& filename,
+                           const std::vector<std::vector<std::vector<std::complex<double>>>>& output3D, size_t nx,
+                           size_t ny, size_t nz, const std::vector<double>& grid_x, const std::vector<double>& grid_y,
+                           const std::vector<double>& grid_z)
+{
+    if (output3D.size() != nx || (nx > 0 && output3D[0].size() != ny) ||
+        (nx > 0 && ny > 0 && output3D[0][0].size() != nz)) {
+        std::cerr << "Error: 3-D matrix dimensions do not match nx, ny, nz" << std::endl;
+        return;
+    }
+    std::vector<std::complex<double>> img(nx * ny * nz);
+    for (size_t x = 0; x < nx; x++)
+        for (size_t y = 0; y < ny; y++)
+            for (size_t z = 0; z < nz; z++) img[(x * ny + y) * nz + z] = output3D[x][y][z];
+    const bool axes = !grid_x.empty() && !grid_y.empty() && !grid_z.empty();
+    if (bsar_image_export(filename.c_str(), reinterpret_cast<const double*>(img.data()), (int64_t)nx, (int64_t)ny,
+                          (int64_t)nz, axes ? grid_x.data() : nullptr, axes ? grid_y.data() : nullptr,
+                          axes ? grid_z.data() : nullptr) != BSAR_OK)
+        std::cerr << "Error: could not write " << filename << std::endl;
+}
+
+ProcessedDEM loadDEM(const std::string& filename)
+{
+    int64_t nx = 0, ny = 0;
+    int32_t flags = 0;
+    if (bsar_dem_load_esri(filename.c_str(), &nx, &ny, nullptr, nullptr, nullptr, &flags) != BSAR_OK)
+        throw std::invalid_argument("bsar: cannot parse the DEM file " + filename);
+    std::vector<double> xv(nx), yv(ny), z((size_t)nx * ny);
+    check_files(bsar_dem_load_esri(filename.c_str(), &nx, &ny, xv.data(), yv.data(), z.data(), &flags), filename);
+    ProcessedDEM d;
+    d.X_vec = xv;
+    d.Y_vec = yv;
+    d.Z_DEM.assign(ny, std::vector<double>(nx));
+    for (int64_t j = 0; j < ny; j++)
+        for (int64_t i = 0; i < nx; i++) d.Z_DEM[j][i] = z[(size_t)j * nx + i];
+    return d;
+}
 
 namespace bsar_compat {
 

@@ -12,7 +12,7 @@ struct DemView {
     int nx, ny;
     int empty;          // X_vec / Y_vec / Z_DEM empty -> height 0
     int asc_x, asc_y;   // axis non-decreasing: binary search finds the reference's first match
-    int uniform;        // both axes strictly ascending (required by the Newton solver)
+    int uniform;        // both axes strictly ascending and equally spaced (required by the Newton solver)
     double x0, y0;      // xv[0], yv[0]
     double stepx, stepy;// (v[n-1] - v[0]) / (n - 1)
 };

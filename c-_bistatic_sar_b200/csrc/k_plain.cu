@@ -47,9 +47,20 @@ __device__ void reflection_point(const DemView& d, double txX, double txY, doubl
     double midY = (txY + rxY) / 2.0;
     double minDist = 1e9, bestZ = 0.0;
     if (!d.empty) {
-        for (int i = 0; i < d.nx; i++) {
+        // every node in scan order; on equally spaced axes only the 3 x 3 nodes around the
+        // nearest one (rounding puts it within one node of the true nearest), scanned in
+        // the same order, so the first minimum is the same node
+        int ia = 0, ib = d.nx - 1, ja = 0, jb = d.ny - 1;
+        if (d.uniform) {
+            const int ci = nearest_node(d.x0, d.stepx, d.nx, midX), cj = nearest_node(d.y0, d.stepy, d.ny, midY);
+            ia = max(ci - 1, 0);
+            ib = min(ci + 1, d.nx - 1);
+            ja = max(cj - 1, 0);
+            jb = min(cj + 1, d.ny - 1);
+        }
+        for (int i = ia; i <= ib; i++) {
             double dx = __ldg(d.xv + i) - midX;
-            for (int j = 0; j < d.ny; j++) {
+            for (int j = ja; j <= jb; j++) {
                 double dy = __ldg(d.yv + j) - midY;
                 double dist = sqrt(dx * dx + dy * dy);
                 if (dist < minDist) {

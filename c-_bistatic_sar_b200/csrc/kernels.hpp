@@ -119,6 +119,10 @@ cudaError_t launch_refraction_mixed(const DemView& d, int pitch, const double* p
                                     double n1, double n2, int W, double* out, cudaStream_t st);
 cudaError_t launch_bp_mixed(const MixedBatch& b, int W, int grid, cudaStream_t st);
 float mixed_start_band(const DemView& d);
+// batched tiled transpose: out[b][c][r] = in[b][r][c] (complex128), and real -> complex128
+cudaError_t launch_transpose_c128(const double2* in, double2* out, int64_t R, int64_t C, int64_t in_ld, int64_t out_ld,
+                                  int64_t in_bs, int64_t out_bs, int64_t batch, cudaStream_t st);
+cudaError_t launch_real_to_c128(const double* in, double2* out, int64_t n, cudaStream_t st);
 int mixed_grid_ctas();   // persistent grid size (SMs x resident CTAs)
 cudaError_t launch_ref_ranges(const DemView& d, const double* tx, const double* rx, int np, const double* center,
                               double n1, double n2, int W, double lambda, double bin_per_m, double* ref_L,

@@ -154,6 +154,26 @@ inline void launched(bsar_ctx* ctx, cudaError_t e, const char* what)
 
 inline void sync(bsar_ctx* ctx) { cuda_check(cudaStreamSynchronize(ctx->stream), "stream synchronize"); }
 
+// Runs an entry point's body with the context locked and its device current, turning
+// errors into a status and the context's last error.
+template <typename F> inline bsar_status guarded(bsar_ctx* ctx, F&& f)
+{
+    if (!ctx) return BSAR_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    try {
+        cuda_check(cudaSetDevice(ctx->device), "cudaSetDevice");
+        f();
+        ctx->last_error.clear();
+        return BSAR_OK;
+    } catch (const Error& e) {
+        ctx->last_error = e.msg;
+        return e.status;
+    } catch (const std::bad_alloc&) {
+        ctx->last_error = "host allocation failed";
+        return BSAR_ERR_OOM_BUDGET;
+    }
+}
+
 // A bounded device-side wait that ran out raises the context's status word.
 inline void check_device_status(bsar_ctx* ctx)
 {
@@ -233,6 +253,18 @@ inline bool strictly_ascending(const double* v, int64_t n)
     return true;
 }
 
+// Strictly ascending and equally spaced: every node within 1e-6 of a step of
+// v[0] + k * step (the node index of a coordinate is then a rounding away).
+inline bool equally_spaced(const double* v, int64_t n)
+{
+    if (!strictly_ascending(v, n)) return false;
+    if (n < 3) return true;
+    const double step = (v[n - 1] - v[0]) / (double)(n - 1);
+    for (int64_t k = 1; k + 1 < n; k++)
+        if (!(std::fabs(v[k] - (v[0] + (double)k * step)) <= 1e-6 * step)) return false;
+    return true;
+}
+
 inline DemDev stage_dem(bsar_ctx* ctx, const bsar_dem* d, bool want_z32)
 {
     check_dem(d);
@@ -261,7 +293,7 @@ inline DemDev stage_dem(bsar_ctx* ctx, const bsar_dem* d, bool want_z32)
     v.z = r.z->as<double>();
     v.asc_x = non_decreasing(d->x_vec, d->nx) ? 1 : 0;
     v.asc_y = non_decreasing(d->y_vec, d->ny) ? 1 : 0;
-    v.uniform = (strictly_ascending(d->x_vec, d->nx) && strictly_ascending(d->y_vec, d->ny)) ? 1 : 0;
+    v.uniform = (equally_spaced(d->x_vec, d->nx) && equally_spaced(d->y_vec, d->ny)) ? 1 : 0;
     v.x0 = d->x_vec[0];
     v.y0 = d->y_vec[0];
     v.stepx = d->nx > 1 ? (d->x_vec[d->nx - 1] - d->x_vec[0]) / (double)(d->nx - 1) : 1.0;
@@ -293,7 +325,7 @@ inline int search_nodes(const DemView& v, double radius)
 inline void check_newton_dem(const DemView& v)
 {
     if (!v.empty && v.nx >= 2 && v.ny >= 2 && !v.uniform)
-        fail(BSAR_ERR_INVALID_ARG, "the Newton solver needs strictly ascending DEM axes");
+        fail(BSAR_ERR_INVALID_ARG, "the Newton solver needs strictly ascending, equally spaced DEM axes");
 }
 
 // ------------------------------------------------------------------------------------

@@ -248,6 +248,62 @@ bsar_status bsar_backproject_mixed_noalloc(bsar_ctx* ctx, bsar_scene_id scene, c
                                            const bsar_bp_opts* opts, double* image_out);
 
 /* ---------------------------------------------------------------------------------
+ * Files around the path.
+ * Matrix files use the reference's binary format (src/binary_reader.cpp:8-99, the
+ * writers of src/data_export.cpp:71-138 and 180-309): uint32 dimension count, uint32
+ * complex flag (1 = complex), uint32 type-name length, char[16] type name, uint64
+ * dimensions, then doubles, real and imaginary interleaved for complex data.
+ * ------------------------------------------------------------------------------- */
+typedef struct bsar_matrix_header {
+    uint32_t ndims;
+    uint32_t is_complex;
+    uint32_t dtype_len;         /* bytes of the type name kept (at most 16) */
+    char dtype[17];             /* type name as stored (not interpreted: values are doubles) */
+    uint64_t dims[8];
+    uint64_t total;             /* product of the dimensions */
+} bsar_matrix_header;
+
+/* readBinary's header (binary_reader.cpp:18-60); BSAR_ERR_NOT_FOUND if the file does not
+ * open, BSAR_ERR_INVALID_ARG if it is truncated. */
+bsar_status bsar_matrix_read_header(const char* path, bsar_matrix_header* out);
+/* readBinary<double> (binary_reader.cpp:8-95): `total` complex128 values into `out`
+ * (real files get a zero imaginary part); fails when capacity < total or the file is short. */
+bsar_status bsar_matrix_read(const char* path, double* out, uint64_t capacity);
+/* exportComplexMatrix (data_export.cpp:71-138) for any rank: header with type "double",
+ * then the values (complex128 when is_complex, else doubles).  Empty matrices are refused. */
+bsar_status bsar_matrix_write(const char* path, uint32_t ndims, const uint64_t* dims, int32_t is_complex,
+                              const double* data);
+
+/* Pulse file -> resident scene.  The file is the 2-D matrix the simulator exports
+ * (dims[0] fast-time samples, dims[1] pulses; the imager's reading,
+ * proc_test_script.cpp:303-331).  desc supplies everything but the samples and
+ * n_samples; desc->n_pulses must equal dims[1].  The values are streamed through pinned
+ * memory to the device; BSAR_FILE_ROW_MAJOR transposes them there. */
+enum { BSAR_FILE_AS_IMAGER = 0,   /* element (sample r, pulse p) at p*dims[0] + r, as the imager indexes it */
+       BSAR_FILE_ROW_MAJOR = 1 }; /* element (r, p) at r*dims[1] + p, the matrix's own row-major layout */
+bsar_status bsar_scene_upload_file(bsar_ctx* ctx, const bsar_scene_desc* desc, const char* path, int32_t layout,
+                                   bsar_scene_id* out);
+
+/* export3DComplexMatrix (data_export.cpp:180-309): image [x][y][z] (z fastest, the layout
+ * bsar_backproject returns) written with x fastest, then y, then z; with all three axes
+ * given, <path without extension>_grid_{x,y,z}.csv beside it as exportVector writes them. */
+bsar_status bsar_image_export(const char* path, const double* image, int64_t nx, int64_t ny, int64_t nz,
+                              const double* gx, const double* gy, const double* gz);
+/* The same from a device image (bsar_backproject_device): permuted on the device. */
+bsar_status bsar_image_export_device(bsar_ctx* ctx, const char* path, const void* d_image, int64_t nx, int64_t ny,
+                                     int64_t nz, const double* gx, const double* gy, const double* gz);
+
+/* loadDEM's ESRI ASCII grid (src/load_dem_simple.cpp:9-224): header keywords ncols,
+ * nrows, xllcorner, yllcorner, cellsize, NODATA_value; the first other line starts the
+ * grid; file row j gives y_vec[j] = yllcorner + j*cellsize (no north-up flip); missing
+ * values read as NODATA.  A .tif name or an unreadable file gives the reference's
+ * stand-in DEM (32 x 32 nodes over [-500, 500]^2 m, height 0) and a flag.  Call with
+ * x_vec = y_vec = z = NULL to get nx, ny; then with buffers of that size (z ny x nx). */
+enum { BSAR_DEM_FALLBACK_TIF = 1, BSAR_DEM_FALLBACK_UNREADABLE = 2, BSAR_DEM_ROWS_MISMATCH = 4 };
+bsar_status bsar_dem_load_esri(const char* path, int64_t* nx, int64_t* ny, double* x_vec, double* y_vec, double* z,
+                               int32_t* flags);
+
+/* ---------------------------------------------------------------------------------
  * Serving: image-formation requests of different grids, pulse counts and DEMs are
  * admitted as they arrive (FIFO) against an HBM budget; each admitted request's scene
  * stays resident while its voxel tiles (128 voxels each) are packed with other requests'

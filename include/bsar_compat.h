@@ -21,6 +21,8 @@
 #define BSAR_COMPAT_H
 
 #include <complex>
+#include <cstddef>
+#include <cstdint>
 #include <string>
 #include <vector>
 
@@ -159,6 +161,28 @@ private:
     static bool isPowerOfTwo(size_t n);
     static size_t nextPowerOfTwo(size_t n);
 };
+
+/* ---------------- include/binary_reader.h:10-31 ---------------------------------- */
+struct MatrixInfo {
+    std::vector<uint64_t> dimensions;
+    bool isComplex;
+    std::string dataType;
+    size_t totalElements;
+};
+template <typename T> std::vector<std::complex<T>> readBinary(const std::string& filename, MatrixInfo& info);
+template <typename T> std::vector<T> readRealBinary(const std::string& filename, MatrixInfo& info);
+
+/* ---------------- include/data_export.h:31-70 ------------------------------------- */
+void exportComplexMatrix(const std::string& filename, const std::vector<std::vector<std::complex<double>>>& data);
+void exportRealMatrix(const std::string& filename, const std::vector<std::vector<double>>& data);
+void exportVector(const std::string& filename, const std::vector<double>& data);
+void export3DComplexMatrix(const std::string& filename,
+                           const std::vector<std::vector<std::vector<std::complex<double>>>>& output3D, size_t nx,
+                           size_t ny, size_t nz, const std::vector<double>& grid_x = {},
+                           const std::vector<double>& grid_y = {}, const std::vector<double>& grid_z = {});
+
+/* ---------------- include/load_dem.h:17 ------------------------------------------- */
+ProcessedDEM loadDEM(const std::string& filename);
 
 /* ---------------- batched imager (no reference counterpart) ----------------------- */
 namespace bsar_compat {

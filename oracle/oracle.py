@@ -218,6 +218,11 @@ class Reference:
         L.ref_fft_correlate_batch.argtypes = [_d, _i64, _i64, _d, _i64, _i32, _i32, _d]
         L.ref_create_chirp.argtypes = [C.c_double] * 4 + [_d, _i64]
         L.ref_create_chirp.restype = _i64
+        L.ref_read_binary.argtypes = [C.c_char_p, C.POINTER(C.c_uint64), C.POINTER(_i32), C.POINTER(_i32), _d, _i64]
+        L.ref_read_binary.restype = _i64
+        L.ref_export_complex_matrix.argtypes = [C.c_char_p, _i64, _i64, _d]
+        L.ref_export_3d.argtypes = [C.c_char_p, _i64, _i64, _i64, _d, _d, _d, _d]
+        L.ref_load_dem.argtypes = [C.c_char_p, C.POINTER(_i64), C.POINTER(_i64), _d, _d, _d]
         L.ref_backproject.argtypes = dem5 + [_d, _d, _i64, _d, _i64, _d, _i64, _d, _i64, _d, _i64,
                                              C.c_double, C.c_double, C.c_double, C.c_double,
                                              C.c_double, _i32, C.POINTER(_i64), _i64, _i32, _d]
@@ -299,3 +304,43 @@ class Reference:
                                n1, n2, c, fs_eff, lam, 0 if legs == "mean" else 1, vp, nv,
                                nthreads, _ptr(out.view(np.float64)))
         return out
+
+
+def _ref_files_methods():
+    """File readers / writers of the reference (binary_reader.cpp, data_export.cpp,
+    load_dem_simple.cpp) on the Reference class."""
+
+    def read_binary(self, path, cap=1 << 26):
+        dims = (C.c_uint64 * 8)()
+        nd, cx = _i32(), _i32()
+        out = np.empty(cap, dtype=np.complex128)
+        n = self.L.ref_read_binary(str(path).encode(), dims, C.byref(nd), C.byref(cx), _ptr(out.view(np.float64)), cap)
+        if n < 0:
+            raise RuntimeError(f"reference readBinary failed on {path}")
+        return out[:n].copy(), [int(dims[k]) for k in range(nd.value)], bool(cx.value)
+
+    def export_complex_matrix(self, path, m):
+        m = np.ascontiguousarray(np.asarray(m, dtype=np.complex128))
+        self.L.ref_export_complex_matrix(str(path).encode(), m.shape[0], m.shape[1], _ptr(m.view(np.float64)))
+
+    def export_3d(self, path, img, gx=None, gy=None, gz=None):
+        img = np.ascontiguousarray(np.asarray(img, dtype=np.complex128))
+        nx, ny, nz = img.shape
+        ax = [None if a is None else _f64(a) for a in (gx, gy, gz)]
+        self.L.ref_export_3d(str(path).encode(), nx, ny, nz, _ptr(img.view(np.float64)),
+                             *[None if a is None else _ptr(a) for a in ax])
+
+    def load_dem(self, path):
+        nx, ny = _i64(), _i64()
+        self.L.ref_load_dem(str(path).encode(), C.byref(nx), C.byref(ny), None, None, None)
+        x = np.empty(max(nx.value, 1))
+        y = np.empty(max(ny.value, 1))
+        z = np.empty(max(nx.value * ny.value, 1))
+        self.L.ref_load_dem(str(path).encode(), C.byref(nx), C.byref(ny), _ptr(x), _ptr(y), _ptr(z))
+        return x[: nx.value], y[: ny.value], z[: nx.value * ny.value].reshape(ny.value, nx.value)
+
+    for f in (read_binary, export_complex_matrix, export_3d, load_dem):
+        setattr(Reference, f.__name__, f)
+
+
+_ref_files_methods()

@@ -1,6 +1,8 @@
 // ref_harness.cpp -- extern "C" entry points over the reference's OWN compiled
-// functions (src/raw_data_processing.cpp, src/fft_utils.cpp, src/interpolation.cpp
-// of DavidAtenciaMondragon/c-_bistatic_sar, compiled unmodified by oracle/Makefile).
+// functions (src/raw_data_processing.cpp, src/fft_utils.cpp, src/interpolation.cpp,
+// and the file readers / writers src/binary_reader.cpp, src/data_export.cpp,
+// src/load_dem_simple.cpp of DavidAtenciaMondragon/c-_bistatic_sar, compiled unmodified
+// by oracle/Makefile).
 //
 // TEST INFRASTRUCTURE ONLY: used to pin the C restatement (bsar_oracle.c), to
 // generate the golden fixtures under tests/golden/, and as the timed CPU
@@ -21,8 +23,11 @@
 #include <omp.h>
 #include <unistd.h>
 
+#include "binary_reader.h"
+#include "data_export.h"
 #include "fft_utils.h"
 #include "interpolation.h"
+#include "load_dem.h"
 #include "raw_data_processing.h"
 
 #ifndef M_PI
@@ -284,6 +289,70 @@ void ref_backproject(int64_t dnx, int64_t dny, const double* xv, const double* y
         out[2 * o] = allPower.real();
         out[2 * o + 1] = allPower.imag();
     }
+}
+
+// readBinary<double> (src/binary_reader.cpp:8-95): returns the element count (-1 on an
+// exception); dims (up to 8), the complex flag and the values (complex128, up to cap).
+int64_t ref_read_binary(const char* path, uint64_t* dims, int32_t* ndims, int32_t* is_complex, double* out,
+                        int64_t cap)
+{
+    try {
+        MatrixInfo info;
+        std::vector<std::complex<double>> v = readBinary<double>(path, info);
+        *ndims = (int32_t)info.dimensions.size();
+        for (size_t k = 0; k < info.dimensions.size() && k < 8; k++) dims[k] = info.dimensions[k];
+        *is_complex = info.isComplex ? 1 : 0;
+        for (int64_t i = 0; i < (int64_t)v.size() && i < cap; i++) {
+            out[2 * i] = v[i].real();
+            out[2 * i + 1] = v[i].imag();
+        }
+        return (int64_t)v.size();
+    } catch (const std::exception&) {
+        return -1;
+    }
+}
+
+// exportComplexMatrix (src/data_export.cpp:71-138) of a rows x cols complex128 matrix.
+void ref_export_complex_matrix(const char* path, int64_t rows, int64_t cols, const double* data)
+{
+    std::vector<std::vector<std::complex<double>>> m(rows, std::vector<std::complex<double>>(cols));
+    for (int64_t i = 0; i < rows; i++)
+        for (int64_t j = 0; j < cols; j++) m[i][j] = {data[2 * (i * cols + j)], data[2 * (i * cols + j) + 1]};
+    exportComplexMatrix(path, m);
+}
+
+// export3DComplexMatrix (src/data_export.cpp:180-309) of an [x][y][z] complex128 image.
+void ref_export_3d(const char* path, int64_t nx, int64_t ny, int64_t nz, const double* img, const double* gx,
+                   const double* gy, const double* gz)
+{
+    std::vector<std::vector<std::vector<std::complex<double>>>> o(
+        nx, std::vector<std::vector<std::complex<double>>>(ny, std::vector<std::complex<double>>(nz)));
+    for (int64_t x = 0; x < nx; x++)
+        for (int64_t y = 0; y < ny; y++)
+            for (int64_t z = 0; z < nz; z++) {
+                const int64_t k = (x * ny + y) * nz + z;
+                o[x][y][z] = {img[2 * k], img[2 * k + 1]};
+            }
+    std::vector<double> ax, ay, az;
+    if (gx) ax.assign(gx, gx + nx);
+    if (gy) ay.assign(gy, gy + ny);
+    if (gz) az.assign(gz, gz + nz);
+    export3DComplexMatrix(path, o, nx, ny, nz, ax, ay, az);
+}
+
+// loadDEM (src/load_dem_simple.cpp:9-224): sizes first (z == NULL), then the arrays
+// (z[j*nx + i] = Z_DEM[j][i]; rows shorter than nx read as 0).
+void ref_load_dem(const char* path, int64_t* nx, int64_t* ny, double* xv, double* yv, double* z)
+{
+    ProcessedDEM d = loadDEM(path);
+    *nx = (int64_t)d.X_vec.size();
+    *ny = (int64_t)d.Y_vec.size();
+    if (!z) return;
+    for (size_t i = 0; i < d.X_vec.size(); i++) xv[i] = d.X_vec[i];
+    for (size_t j = 0; j < d.Y_vec.size(); j++) yv[j] = d.Y_vec[j];
+    for (size_t j = 0; j < d.Y_vec.size(); j++)
+        for (size_t i = 0; i < d.X_vec.size(); i++)
+            z[j * d.X_vec.size() + i] = (j < d.Z_DEM.size() && i < d.Z_DEM[j].size()) ? d.Z_DEM[j][i] : 0.0;
 }
 
 }  // extern "C"

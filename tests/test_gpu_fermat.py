@@ -96,3 +96,27 @@ def test_mixed_crossings_match_fp64(ctx, sc2):
     dl = np.abs(L(T, x32, P, sp.n1, sp.n2) - L(T, x64, P, sp.n1, sp.n2))
     assert dl.max() <= 1e-5
     assert np.mean(np.linalg.norm(x32 - x64, axis=1) <= 1e-4) >= 0.999
+
+
+def test_reflection_points_nearest_node_lookup(ctx, reference, sc1):
+    """calculateReflectionPoint (src/raw_data_processing.cpp:575-609) on the GPU: on
+    equally spaced axes only the 3 x 3 nodes around the rounded nearest node are scanned;
+    the result equals the reference's full scan bit for bit, for midpoints inside and
+    outside the DEM, on nodes and exactly half-way between them."""
+    x, y = sc1.x_vec, sc1.y_vec
+    dx = x[1] - x[0]
+    rng = np.random.default_rng(21)
+    n = 3000
+    mids = np.stack([rng.uniform(x[0] - 20, x[-1] + 20, n), rng.uniform(y[0] - 20, y[-1] + 20, n)], 1)
+    k = rng.integers(0, len(x) - 1, 400)
+    mids[:200, 0] = x[k[:200]] + 0.5 * dx              # half-way between nodes
+    mids[200:400] = np.stack([x[k[200:]], y[k[200:] % len(y)]], 1)   # on nodes
+    off = rng.normal(size=(n, 2)) * 3.0
+    off[:400] = 0.0                                    # so the midpoint is exactly `mids`
+    T = np.concatenate([mids - off, np.full((n, 1), 30.0)], 1)
+    R = np.concatenate([mids + off, np.full((n, 1), 30.0)], 1)
+    P = [x[len(x) // 2], y[len(y) // 2], -4.0]
+    sp = sc1.spec
+    g = ctx.slant_range_fermat(bsar.DemArrays(x, y, sc1.z), T, R, P, sp.n1, sp.n2, solver="grid", reflection=True)
+    r = reference.slant_range_fermat(O.Dem(x, y, sc1.z), T, R, P, sp.n1, sp.n2)
+    assert np.array_equal(g[3], r[3])
