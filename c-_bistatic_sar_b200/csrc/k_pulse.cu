@@ -45,30 +45,73 @@ template <typename V> __device__ __forceinline__ V csub(V a, V b) { V r; r.x = a
 template <typename V> __device__ __forceinline__ V cconj(V a) { a.y = -a.y; return a; }
 
 // In-place radix-2 DIF over smem x[0..P): natural order in, bit-reversed order out.
-// tw[k] = exp(-2 pi i k / P), k < P/2.
+// tw[k] = exp(-2 pi i k / P), k < P/2.  Stages run in pairs: each thread takes the four
+// elements two consecutive stages combine and does both stages' butterflies in
+// registers (the same operations, so the same bits, as two radix-2 passes), halving the
+// shared-memory round trips and barriers.
 template <typename V>
 __device__ __forceinline__ void fft_dif(V* x, int P, int logP, const V* __restrict__ tw)
 {
-    for (int s = logP - 1; s >= 0; s--) {
-        const int h = 1 << s;            // half span
-        const int tstride = P >> (s + 1); // twiddle index step
+    int s = logP - 1;
+    for (; s >= 1; s -= 2) {
+        const int h2 = 1 << (s - 1), h = h2 << 1;
+        const int ts = P >> (s + 1), ts2 = ts << 1;
+        for (int q = threadIdx.x; q < (P >> 2); q += blockDim.x) {
+            const int k2 = q & (h2 - 1);
+            const int e0 = ((q >> (s - 1)) << (s + 1)) + k2;
+            V a0 = x[e0], a1 = x[e0 + h2], a2 = x[e0 + h], a3 = x[e0 + h + h2];
+            // stage s: (e0, e2) with twiddle k2, (e1, e3) with twiddle k2 + h2
+            V b0 = cadd(a0, a2), b2 = cmul(csub(a0, a2), __ldg(tw + k2 * ts));
+            V b1 = cadd(a1, a3), b3 = cmul(csub(a1, a3), __ldg(tw + (k2 + h2) * ts));
+            // stage s - 1: (e0, e1) and (e2, e3), twiddle k2
+            const V w = __ldg(tw + k2 * ts2);
+            x[e0] = cadd(b0, b1);
+            x[e0 + h2] = cmul(csub(b0, b1), w);
+            x[e0 + h] = cadd(b2, b3);
+            x[e0 + h + h2] = cmul(csub(b2, b3), w);
+        }
+        __syncthreads();
+    }
+    if (s == 0) {
         for (int b = threadIdx.x; b < (P >> 1); b += blockDim.x) {
-            int k = b & (h - 1);
-            int i0 = ((b >> s) << (s + 1)) + k;
-            int i1 = i0 + h;
-            V a = x[i0], c = x[i1];
-            x[i0] = cadd(a, c);
-            x[i1] = cmul(csub(a, c), __ldg(tw + k * tstride));
+            V a = x[2 * b], c = x[2 * b + 1];
+            x[2 * b] = cadd(a, c);
+            x[2 * b + 1] = cmul(csub(a, c), __ldg(tw));
         }
         __syncthreads();
     }
 }
 
-// In-place radix-2 DIT over smem x[0..P): bit-reversed order in, natural order out.
+// In-place radix-2 DIT over smem x[0..P): bit-reversed order in, natural order out,
+// stages paired in registers as in fft_dif.
 template <typename V>
 __device__ __forceinline__ void fft_dit(V* x, int P, int logP, const V* __restrict__ tw)
 {
-    for (int s = 0; s < logP; s++) {
+    int s = 0;
+    for (; s + 1 < logP; s += 2) {
+        const int h = 1 << s;
+        const int ts = P >> (s + 1), ts2 = ts >> 1;
+        for (int q = threadIdx.x; q < (P >> 2); q += blockDim.x) {
+            const int k = q & (h - 1);
+            const int e0 = ((q >> s) << (s + 2)) + k;
+            V a0 = x[e0], a1 = x[e0 + h], a2 = x[e0 + 2 * h], a3 = x[e0 + 3 * h];
+            // stage s: (e0, e1) and (e2, e3), twiddle k
+            const V w = __ldg(tw + k * ts);
+            V t = cmul(a1, w);
+            V b0 = cadd(a0, t), b1 = csub(a0, t);
+            t = cmul(a3, w);
+            V b2 = cadd(a2, t), b3 = csub(a2, t);
+            // stage s + 1: (e0, e2) with twiddle k, (e1, e3) with twiddle k + h
+            t = cmul(b2, __ldg(tw + k * ts2));
+            x[e0] = cadd(b0, t);
+            x[e0 + 2 * h] = csub(b0, t);
+            t = cmul(b3, __ldg(tw + (k + h) * ts2));
+            x[e0 + h] = cadd(b1, t);
+            x[e0 + 3 * h] = csub(b1, t);
+        }
+        __syncthreads();
+    }
+    if (s < logP) {
         const int h = 1 << s;
         const int tstride = P >> (s + 1);
         for (int b = threadIdx.x; b < (P >> 1); b += blockDim.x) {
@@ -146,6 +189,40 @@ __device__ __forceinline__ double hermite_comp(const Hermite& H, int64_t n, doub
     return H.h1 * p0 + H.h2 * p1 + H.h3 * dPrev + H.h4 * dNext;
 }
 
+// Hermite upsampling into FP32 storage (complex64, or FP16 complex x 1/scale): one
+// thread per input interval computes the interval's `factor` outputs from one read of
+// its four neighbours, with the weights of t = k / factor (FP64 formula rounded to FP32).
+// The last interval repeats the last sample, as splineInterpolation's clamp to interval
+// n - 2 with t = 1 does.  `ld(i)` returns sample i as float2.
+template <typename Load>
+__device__ __forceinline__ void hermite_store32(Load ld, int64_t n, int factor, int out_kind, float inv_scale,
+                                                float2* __restrict__ out32, __half2* __restrict__ out16)
+{
+    for (int64_t iv = threadIdx.x; iv < n; iv += blockDim.x) {
+        const int64_t o0 = iv * factor;
+        if (iv >= n - 1) {
+            const float2 v = ld(n - 1);
+            for (int k = 0; k < factor; k++) {
+                if (out_kind == 1) out32[o0 + k] = v;
+                else out16[o0 + k] = __floats2half2_rn(v.x * inv_scale, v.y * inv_scale);
+            }
+            continue;
+        }
+        const float2 pm1 = ld(iv > 0 ? iv - 1 : 0), p0 = ld(iv), p1 = ld(iv + 1), p2 = ld(iv + 2 < n ? iv + 2 : n - 1);
+        const float dpx = iv > 0 ? p0.x - pm1.x : 0.f, dpy = iv > 0 ? p0.y - pm1.y : 0.f;
+        const float dnx = iv < n - 2 ? p2.x - p1.x : 0.f, dny = iv < n - 2 ? p2.y - p1.y : 0.f;
+        for (int k = 0; k < factor; k++) {
+            const double t = (double)k / factor, t2 = t * t, t3 = t2 * t;
+            const float h1 = (float)(2 * t3 - 3 * t2 + 1), h2 = (float)(-2 * t3 + 3 * t2);
+            const float h3 = (float)(t3 - 2 * t2 + t), h4 = (float)(t3 - t2);
+            const float re = fmaf(h1, p0.x, fmaf(h2, p1.x, fmaf(h3, dpx, h4 * dnx)));
+            const float im = fmaf(h1, p0.y, fmaf(h2, p1.y, fmaf(h3, dpy, h4 * dny)));
+            if (out_kind == 1) out32[o0 + k] = make_float2(re, im);
+            else out16[o0 + k] = __floats2half2_rn(re * inv_scale, im * inv_scale);
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------------
 // Pulse compression (+ optional upsampling) of `batch` pulses, one CTA per pulse.
 //   in        batch x ns complex128 (raw echoes), zero-padded to P
@@ -211,6 +288,11 @@ __global__ void k_pulse_compress(const double2* __restrict__ in, int ns, int P, 
         if (threadIdx.x == 0) scale16[p] = scale;
     }
     const float inv_scale = 1.0f / scale;
+    if (out_kind != 0) {
+        hermite_store32([&](int64_t i) { const V v = x[i]; return make_float2((float)v.x, (float)v.y); }, n, factor,
+                        out_kind, inv_scale, out32 ? out32 + p * nout : nullptr, out16 ? out16 + p * nout : nullptr);
+        return;
+    }
     for (int64_t o = threadIdx.x; o < nout; o += blockDim.x) {
         Hermite H = hermite_at(o, n, factor);
         int64_t i = H.idx;
@@ -257,18 +339,8 @@ __global__ void k_upsample_store(const double2* __restrict__ in, int64_t n, int 
         if (threadIdx.x == 0) scale16[p] = scale;
     }
     const float inv_scale = 1.0f / scale;
-    for (int64_t o = threadIdx.x; o < nout; o += blockDim.x) {
-        Hermite H = hermite_at(o, n, factor);
-        int64_t i = H.idx;
-        double2 pm1 = __ldg(src + (i > 0 ? i - 1 : 0)), p0 = __ldg(src + i), p1 = __ldg(src + i + 1);
-        double2 p2 = __ldg(src + (i + 2 < n ? i + 2 : n - 1));
-        double re = hermite_comp(H, n, pm1.x, p0.x, p1.x, p2.x);
-        double im = hermite_comp(H, n, pm1.y, p0.y, p1.y, p2.y);
-        if (out_kind == 1)
-            out32[p * nout + o] = make_float2((float)re, (float)im);
-        else
-            out16[p * nout + o] = __floats2half2_rn((float)re * inv_scale, (float)im * inv_scale);
-    }
+    hermite_store32([&](int64_t i) { const double2 v = __ldg(src + i); return make_float2((float)v.x, (float)v.y); }, n,
+                    factor, out_kind, inv_scale, out32 ? out32 + p * nout : nullptr, out16 ? out16 + p * nout : nullptr);
 }
 
 // Plain batched FFT rows (natural order in and out) -- FFTProcessor::fft / ::ifft.
