@@ -237,7 +237,7 @@ def cpu_reference_rate(sc, seconds: float, threads: int, use_ref: bool = True, z
         "values": last["vals"]}
 
 
-def serve_leg(ctx, torch, n_requests: int, burst: int, fp64_sample: int, load: float = 0.8):
+def serve_leg(ctx, torch, n_requests: int, burst: int, fp64_sample: int, load: float = 0.8, tiles: int = 0):
     """Served mixed workload through bsar_server_* (see the module docstring)."""
     import bsar
     from bsar import scene as S
@@ -258,10 +258,11 @@ def serve_leg(ctx, torch, n_requests: int, burst: int, fp64_sample: int, load: f
                           chirp_T=sp.pulse_T, precision="mixed")
 
     budget = 120 * 10**9
-    out = {"requests": n_requests, "hbm_budget_bytes": budget, "total_voxel_pulses": float(vp.sum())}
+    out = {"requests": n_requests, "hbm_budget_bytes": budget, "total_voxel_pulses": float(vp.sum()),
+           "tiles_per_launch": tiles or "two waves of resident CTAs"}
     # closed burst: capacity of the server on this mix
     burst = min(burst, n_requests)
-    with bsar.Server(ctx, hbm_budget_bytes=budget) as srv:
+    with bsar.Server(ctx, hbm_budget_bytes=budget, tiles_per_launch=tiles) as srv:
         submit(srv, 0)
         srv.wait(1)                                            # warm-up (graph capture, first admission)
         t = time.perf_counter()
@@ -276,7 +277,7 @@ def serve_leg(ctx, torch, n_requests: int, burst: int, fp64_sample: int, load: f
     # open loop: Poisson arrivals at `load` x capacity
     arrivals = S.poisson_arrivals(n_requests, rate)
     with ClockSampler(torch.cuda.current_device()) as clk:
-        with bsar.Server(ctx, hbm_budget_bytes=budget) as srv:
+        with bsar.Server(ctx, hbm_budget_bytes=budget, tiles_per_launch=tiles) as srv:
             submit(srv, 0)
             srv.wait(1)
             t0 = time.perf_counter()
@@ -295,6 +296,10 @@ def serve_leg(ctx, torch, n_requests: int, burst: int, fp64_sample: int, load: f
                      "mean_ms": float(lat.mean()), "max_ms": float(lat.max()), "launches": int(st["launches"]),
                      "tiles": int(st["tiles"]), "peak_inflight": int(st["peak_inflight"]),
                      "peak_reserved_gb": st["peak_reserved_bytes"] / 1e9, "failed": int(st["failed"])}
+    # a request cannot finish sooner than its own work at the full measured capacity
+    floor_ms = np.sort(vp / cap_vps * 1e3)
+    out["served"]["p99_service_floor_ms"] = float(np.percentile(floor_ms, 99))
+    out["served"]["p50_service_floor_ms"] = float(np.percentile(floor_ms, 50))
     out["clocks"] = clk.summary()
     # the same requests one after another in the plain FP64 form (a spread sample)
     idx = np.linspace(0, n_requests - 1, min(fp64_sample, n_requests)).astype(int)
@@ -372,6 +377,7 @@ def main():
     ap.add_argument("--serve-burst", type=int, default=64, help="requests of the capacity burst")
     ap.add_argument("--serve-fp64-sample", type=int, default=24, help="requests run serially in FP64")
     ap.add_argument("--serve-only", action="store_true", help="only the served workload")
+    ap.add_argument("--serve-tiles", type=int, default=0, help="work items per launch (0: two waves of CTAs)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -394,7 +400,8 @@ def main():
 
     if args.serve_only:
         ctx = bsar.Context(local)
-        res = serve_leg(ctx, torch, args.serve_requests, args.serve_burst, args.serve_fp64_sample)
+        res = serve_leg(ctx, torch, args.serve_requests, args.serve_burst, args.serve_fp64_sample,
+                        tiles=args.serve_tiles)
         if rank == 0:
             print(json.dumps({"serving": res}), flush=True)
         ctx.close()
@@ -505,13 +512,19 @@ def main():
         vi = rng.integers(0, [sp.nx, sp.ny, sp.nz], size=(1 << 16, 3))
         P = np.stack([sc.gx[vi[:, 0]], sc.gy[vi[:, 1]], sc.gz[vi[:, 2]]], axis=1)
         demA = bsar.DemArrays(sc.x_vec, sc.y_vec, sc.z)
-        cross = 0.0
+        cross = dpath = 0.0
         for ant, na, nb, first in ((sc.tx, sp.n1, sp.n2, True), (sc.rx, sp.n2, sp.n1, False)):
             p1, p2 = (ant[pi], P) if first else (P, ant[pi])
             x64 = ctx.refraction_points(demA, p1, p2, na, nb, solver="newton")
             x32 = ctx.refraction_points(demA, p1, p2, na, nb, solver="newton", precision="mixed")
             cross = max(cross, float(np.linalg.norm(x32 - x64, axis=1).max()))
+
+            def path(X):
+                return na * np.linalg.norm(p1 - X, axis=1) + nb * np.linalg.norm(p2 - X, axis=1)
+
+            dpath = max(dpath, float(np.abs(path(x32) - path(x64)).max()))
         acc["mixed_fermat_crossing_max_err_m"] = cross
+        acc["mixed_fermat_path_max_err_m"] = dpath
         acc["fermat_sample"] = "65536 random (pulse, voxel) pairs per leg, Tx->voxel and voxel->Rx"
 
     # ---------------- roofline of the dominant kernel (k_bp_mixed) ------------------
@@ -529,7 +542,9 @@ def main():
                 "kernel": "k_bp_mixed", "kernel_ms": bp_avg_ms,
                 "peak_source": f"nominal 148 SM x 128 FP32 lanes x 2 flop x {sm_mhz:.0f} MHz (no FP32-pipe "
                                f"figure in MEASURED_PEAKS.json)",
-                "sfu": {"achieved_gops": sfu_rate / 1e9, "peak_gops": sfu_peak / 1e9, "frac": sfu_rate / sfu_peak},
+                "sfu": {"achieved_gops": sfu_rate / 1e9, "peak_gops": sfu_peak / 1e9, "frac": sfu_rate / sfu_peak,
+                        "note": "algorithmic count (both legs' rsqrt per scanned node); the warp's shared E-leg "
+                                "table executes about half of them"},
                 "gather": {"bytes_per_voxel_pulse": 16, "achieved_gbs": 16 * vp / (bp_avg_ms / 1e3) / 1e9,
                            "hbm_peak_gbs": peaks.get("hbm_gbs"), "peak_source": peak_src},
                 "fp32_flops_per_voxel_pulse": fp32_flops_per_voxel_pulse(W), "node_scan_half_width": W}
@@ -570,7 +585,8 @@ def main():
     serving = None
     if rank == 0 and world == 1 and args.serve_requests > 0:
         ctx.set_stream(None)
-        serving = serve_leg(ctx, torch, args.serve_requests, args.serve_burst, args.serve_fp64_sample)
+        serving = serve_leg(ctx, torch, args.serve_requests, args.serve_burst, args.serve_fp64_sample,
+                            tiles=args.serve_tiles)
 
     if rank == 0:
         line = {

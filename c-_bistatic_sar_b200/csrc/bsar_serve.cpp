@@ -524,9 +524,13 @@ bsar_status bsar_server_create(bsar_ctx* ctx, const bsar_server_opts* opts, bsar
             uint64_t keep = ~0ull;     // keep freed blocks for the next admission
             cuda_check(cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep), "pool attribute");
         }
-        cuda_check(cudaStreamCreateWithFlags(&s->io, cudaStreamNonBlocking), "stream");
+        // admission outranks the batches: its kernels take the SM slots the batch CTAs
+        // free before the queued batch does, so a request is ready for the next batch
+        int least = 0, greatest = 0;
+        cuda_check(cudaDeviceGetStreamPriorityRange(&least, &greatest), "stream priorities");
+        cuda_check(cudaStreamCreateWithPriority(&s->io, cudaStreamNonBlocking, greatest), "stream");
         for (ServeBatch& bt : s->batch) {
-            cuda_check(cudaStreamCreateWithFlags(&bt.st, cudaStreamNonBlocking), "stream");
+            cuda_check(cudaStreamCreateWithPriority(&bt.st, cudaStreamNonBlocking, least), "stream");
             cuda_check(cudaEventCreateWithFlags(&bt.ev, cudaEventDisableTiming), "event");
             cuda_check(cudaMallocHost((void**)&bt.h_reqs, sizeof(MixedReq) * kMaxSlots), "pinned");
             cuda_check(cudaMallocHost((void**)&bt.h_tiles, sizeof(int2) * s->max_tiles), "pinned");
