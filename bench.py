@@ -450,12 +450,15 @@ def main():
     raw_pinned.numpy()[...] = sc.raw
     dem = bsar.DemArrays(sc.x_vec, sc.y_vec, sc.z)
     f0, f1 = -sp.bandwidth / 2, sp.bandwidth / 2
-    img_host = np.empty((sp.nx, sp.ny, sp.nz), dtype=np.complex128)
+    # the image lands in pinned host memory
+    img_pinned = torch.empty((sp.nx, sp.ny, sp.nz), dtype=torch.complex128, pin_memory=True)
+    img_host = img_pinned.numpy()
 
     def e2e_step():
         s = ctx.scene_upload(dem, sc.tx, sc.rx, raw_pinned.numpy(), upsample=sp.upsample, n1=sp.n1, n2=sp.n2,
                              c=3e8, fc=sp.fc, fs=sp.fs, chirp_f0=f0, chirp_f1=f1, chirp_T=sp.pulse_T)
-        out = ctx.backproject(s, sc.gx, sc.gy, sc.gz, solver="newton", legs="per_pulse", precision="mixed")
+        out = ctx.backproject(s, sc.gx, sc.gy, sc.gz, solver="newton", legs="per_pulse", precision="mixed",
+                              out=img_host)
         ctx.scene_release(s)
         return out
 
@@ -464,11 +467,12 @@ def main():
         e2e_step()
     torch.cuda.synchronize()
     barrier()
-    t = time.perf_counter()
-    for _ in range(e2e_steps):
-        img_host = e2e_step()
-    torch.cuda.synchronize()
-    e2e_s = max_over_ranks((time.perf_counter() - t) / e2e_steps)
+    with ClockSampler(local) as clk_e2e:
+        t = time.perf_counter()
+        for _ in range(e2e_steps):
+            img_host = e2e_step()
+        torch.cuda.synchronize()
+        e2e_s = max_over_ranks((time.perf_counter() - t) / e2e_steps)
     barrier()
     h2d = (sc.raw.nbytes + sc.tx.nbytes + sc.rx.nbytes + sc.x_vec.nbytes + sc.y_vec.nbytes + sc.z.nbytes
            + 8 * (len(sc.gx) + len(sc.gy) + len(sc.gz)))
@@ -603,7 +607,8 @@ def main():
                              f"{sp.n_pulses * sp.n_samples * sp.upsample * 8 / 2**20:.0f} MiB)",
                        "parallelism": f"voxel slabs x{world}, no collective"},
             "e2e": {"value": world * vp / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_s * 1e3},
+                    "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_s * 1e3, "clocks": clk_e2e.summary(),
+                    "host_buffers": "pinned (raw pulses in, image out)"},
             "gpu_launches": int(launches),
             "roofline": roofline,
             "forms": forms,

@@ -363,10 +363,15 @@ class Context:
         return (gx, gy, gz), Grid(len(gx), len(gy), len(gz), _p(gx), _p(gy), _p(gz))
 
     def backproject(self, sid: int, gx, gy, gz, *, solver="grid", legs="mean", precision="fp64",
-                    search_radius_m=0.0):
+                    search_radius_m=0.0, out=None):
+        """Image [x][y][z] complex128; `out` (C-contiguous complex128 of that shape, e.g.
+        a view of pinned memory) receives it instead of a new array."""
         keep, g = self._grid(gx, gy, gz)
         o = BpOpts(SOLVER[solver], LEGS[legs], PRECISION[precision], 0, search_radius_m)
-        out = np.empty((g.nx, g.ny, g.nz), dtype=np.complex128)
+        if out is None:
+            out = np.empty((g.nx, g.ny, g.nz), dtype=np.complex128)
+        elif out.shape != (g.nx, g.ny, g.nz) or out.dtype != np.complex128 or not out.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous complex128 array of the grid's shape")
         self._ok(self.L.bsar_backproject(self.h, sid, C.byref(g), C.byref(o), _p(out.view(np.float64))))
         return out
 

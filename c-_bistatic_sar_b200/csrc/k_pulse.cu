@@ -198,6 +198,13 @@ template <typename Load>
 __device__ __forceinline__ void hermite_store32(Load ld, int64_t n, int factor, int out_kind, float inv_scale,
                                                 float2* __restrict__ out32, __half2* __restrict__ out16)
 {
+    __shared__ float4 wt[64];                       // weights of t = k / factor (factor <= 64)
+    if (threadIdx.x < factor) {
+        const double t = (double)threadIdx.x / factor, t2 = t * t, t3 = t2 * t;
+        wt[threadIdx.x] = make_float4((float)(2 * t3 - 3 * t2 + 1), (float)(-2 * t3 + 3 * t2),
+                                      (float)(t3 - 2 * t2 + t), (float)(t3 - t2));
+    }
+    __syncthreads();
     for (int64_t iv = threadIdx.x; iv < n; iv += blockDim.x) {
         const int64_t o0 = iv * factor;
         if (iv >= n - 1) {
@@ -212,9 +219,8 @@ __device__ __forceinline__ void hermite_store32(Load ld, int64_t n, int factor, 
         const float dpx = iv > 0 ? p0.x - pm1.x : 0.f, dpy = iv > 0 ? p0.y - pm1.y : 0.f;
         const float dnx = iv < n - 2 ? p2.x - p1.x : 0.f, dny = iv < n - 2 ? p2.y - p1.y : 0.f;
         for (int k = 0; k < factor; k++) {
-            const double t = (double)k / factor, t2 = t * t, t3 = t2 * t;
-            const float h1 = (float)(2 * t3 - 3 * t2 + 1), h2 = (float)(-2 * t3 + 3 * t2);
-            const float h3 = (float)(t3 - 2 * t2 + t), h4 = (float)(t3 - t2);
+            const float4 w = wt[k];
+            const float h1 = w.x, h2 = w.y, h3 = w.z, h4 = w.w;
             const float re = fmaf(h1, p0.x, fmaf(h2, p1.x, fmaf(h3, dpx, h4 * dnx)));
             const float im = fmaf(h1, p0.y, fmaf(h2, p1.y, fmaf(h3, dpy, h4 * dny)));
             if (out_kind == 1) out32[o0 + k] = make_float2(re, im);
@@ -244,10 +250,24 @@ __global__ void k_pulse_compress(const double2* __restrict__ in, int ns, int P, 
     __shared__ float red[32];
     const int64_t p = blockIdx.x;
     const double2* __restrict__ src = in + p * (int64_t)ns;
-    for (int i = threadIdx.x; i < P; i += blockDim.x) {
-        V v;
-        if (i < ns) { double2 d = __ldg(src + i); v.x = (R)d.x; v.y = (R)d.y; } else { v.x = 0; v.y = 0; }
-        x[i] = v;
+    // four loads in flight per thread before the shared-memory stores
+    for (int i0 = threadIdx.x; i0 < P; i0 += 4 * blockDim.x) {
+        double2 d[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int i = i0 + u * blockDim.x;
+            d[u] = (i < ns) ? __ldg(src + i) : make_double2(0.0, 0.0);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int i = i0 + u * blockDim.x;
+            if (i < P) {
+                V v;
+                v.x = (R)d[u].x;
+                v.y = (R)d[u].y;
+                x[i] = v;
+            }
+        }
     }
     __syncthreads();
     fft_dif(x, P, logP, tw);
@@ -703,12 +723,14 @@ cudaError_t launch_pulse_compress(const PulseArgs& a, cudaStream_t st)
     if (a.real_bytes == 8) {
         size_t sm = fft_smem_bytes<double>(a.P);
         cudaFuncSetAttribute(k_pulse_compress<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        cudaFuncSetAttribute(k_pulse_compress<double>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         k_pulse_compress<double><<<(unsigned)a.batch, fft_threads(a.P), sm, st>>>(
             a.in, a.ns, a.P, a.logP, (const double2*)a.tw, (const double2*)a.spec, a.n_keep, a.factor,
             a.out_kind, a.out64, a.out32, a.out16, a.scale16);
     } else {
         size_t sm = fft_smem_bytes<float>(a.P);
         cudaFuncSetAttribute(k_pulse_compress<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        cudaFuncSetAttribute(k_pulse_compress<float>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         k_pulse_compress<float><<<(unsigned)a.batch, fft_threads(a.P), sm, st>>>(
             a.in, a.ns, a.P, a.logP, (const float2*)a.tw, (const float2*)a.spec, a.n_keep, a.factor,
             a.out_kind, a.out64, a.out32, a.out16, a.scale16);
