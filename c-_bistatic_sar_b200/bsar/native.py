@@ -129,6 +129,8 @@ def lib() -> C.CDLL:
         "bsar_scene_release": ([V, C.c_uint64], _i32),
         "bsar_scene_synthesize": ([V, C.POINTER(SceneDesc), _d, _d, _i64, C.c_double, C.c_uint64,
                                    C.POINTER(C.c_uint64)], _i32),
+        "bsar_scene_synthesize_ex": ([V, C.POINTER(SceneDesc), _d, _d, _i64, C.c_double, C.c_uint64, _i32,
+                                      C.POINTER(C.c_uint64)], _i32),
         "bsar_scene_read_samples": ([V, C.c_uint64, _d], _i32),
         "bsar_scene_compress": ([V, C.c_uint64, _i32], _i32),
         "bsar_scene_read_upsampled": ([V, C.c_uint64, _d], _i32),
@@ -303,8 +305,9 @@ class Context:
 
     def scene_synthesize(self, dem: DemArrays, tx, rx, n_samples, scat_pos, scat_amp, *, snr_db=float("inf"),
                          seed=0, upsample=4, n1=1.0, n2=2.0, c=3e8, fc=1e9, fs=1.2e9, chirp_f0=0.0, chirp_f1=0.0,
-                         chirp_T=0.0) -> int:
-        """Resident raw scene with echoes synthesised on the device (bsar_scene_synthesize)."""
+                         chirp_T=0.0, reference_bins=False) -> int:
+        """Resident raw scene with echoes synthesised on the device (bsar_scene_synthesize);
+        reference_bins: the simulator's integer echo bin and circular wrap."""
         tx = _f64(tx, (-1, 3))
         rx = _f64(rx, (-1, 3))
         pos = _f64(scat_pos, (-1, 3))
@@ -312,8 +315,8 @@ class Context:
         desc = SceneDesc(dem.c, len(tx), _p(tx), _p(rx), int(n_samples), None, 0, upsample, n1, n2, c, fc, fs,
                          chirp_f0, chirp_f1, chirp_T)
         sid = C.c_uint64()
-        self._ok(self.L.bsar_scene_synthesize(self.h, C.byref(desc), _p(pos), _p(amp), len(amp), snr_db,
-                                              seed & (2**64 - 1), C.byref(sid)))
+        self._ok(self.L.bsar_scene_synthesize_ex(self.h, C.byref(desc), _p(pos), _p(amp), len(amp), snr_db,
+                                                 seed & (2**64 - 1), 1 if reference_bins else 0, C.byref(sid)))
         return int(sid.value)
 
     def scene_upload_file(self, dem: DemArrays, tx, rx, path, *, layout="as_imager", kind="compressed", upsample=4,

@@ -278,9 +278,9 @@ bsar_status bsar_scene_upload(bsar_ctx* ctx, const bsar_scene_desc* desc, bsar_s
     });
 }
 
-bsar_status bsar_scene_synthesize(bsar_ctx* ctx, const bsar_scene_desc* desc, const double* scat_pos,
-                                  const double* scat_amp, int64_t n_scat, double snr_db, uint64_t seed,
-                                  bsar_scene_id* out)
+bsar_status bsar_scene_synthesize_ex(bsar_ctx* ctx, const bsar_scene_desc* desc, const double* scat_pos,
+                                     const double* scat_amp, int64_t n_scat, double snr_db, uint64_t seed, int32_t flags,
+                                     bsar_scene_id* out)
 {
     return guarded(ctx, [&] {
         if (!desc || !out) fail(BSAR_ERR_INVALID_ARG, "NULL argument");
@@ -289,10 +289,18 @@ bsar_status bsar_scene_synthesize(bsar_ctx* ctx, const bsar_scene_desc* desc, co
         if (!all_finite(scat_pos, 3 * n_scat) || !all_finite(scat_amp, n_scat))
             fail(BSAR_ERR_INVALID_ARG, "non-finite scatterer");
         auto sc = make_scene(ctx, *desc, false);
-        synthesize_samples(ctx, sc.get(), scat_pos, scat_amp, n_scat, snr_db, seed);
+        if (flags & ~BSAR_SYNTH_REFERENCE_BINS) fail(BSAR_ERR_INVALID_ARG, "unknown synthesis flags");
+        synthesize_samples(ctx, sc.get(), scat_pos, scat_amp, n_scat, snr_db, seed, flags);
         sync(ctx);
         *out = add_scene(ctx, std::move(sc));
     });
+}
+
+bsar_status bsar_scene_synthesize(bsar_ctx* ctx, const bsar_scene_desc* desc, const double* scat_pos,
+                                  const double* scat_amp, int64_t n_scat, double snr_db, uint64_t seed,
+                                  bsar_scene_id* out)
+{
+    return bsar_scene_synthesize_ex(ctx, desc, scat_pos, scat_amp, n_scat, snr_db, seed, 0, out);
 }
 
 bsar_status bsar_scene_read_samples(bsar_ctx* ctx, bsar_scene_id id, double* out)

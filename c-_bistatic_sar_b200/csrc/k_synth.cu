@@ -10,6 +10,11 @@
 //                  convention, at the exact fractional delay), plus complex Gaussian
 //                  noise from a counter-based generator (splitmix64 + Box-Muller)
 //
+// With `ref_bins` the envelope follows the simulator exactly instead: the echo's chirp is
+// centred on sample 1 + round(t * fs) (src/raw_data_processing.cpp:329) and wraps around
+// the pulse as its circular convolution with the fftshifted chirp does (:371-406); the
+// carrier phase stays exact in both modes.
+//
 // Compiled with --fmad=false like the other FP64 translation units.
 #include <cuda_runtime.h>
 
@@ -22,8 +27,8 @@ namespace bsar {
 
 __global__ void k_echo_paths(DemView d, const double* __restrict__ tx, const double* __restrict__ rx, int np,
                              const double* __restrict__ spos, const double* __restrict__ samp, int ns_, double n1,
-                             double n2, int W, double c, double fc, double* __restrict__ tau,
-                             double2* __restrict__ carrier)
+                             double n2, int W, double c, double fc, double fs, int ref_bins,
+                             double* __restrict__ tau, double2* __restrict__ carrier)
 {
     const int64_t total = (int64_t)np * ns_;
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total; k += (int64_t)gridDim.x * blockDim.x) {
@@ -39,7 +44,8 @@ __global__ void k_echo_paths(DemView d, const double* __restrict__ tx, const dou
             return sqrt(x * x + y * y + z * z);
         };
         const double L = n1 * dist(T, a) + n2 * dist(P, a) + n2 * dist(P, b) + n1 * dist(R, b);
-        tau[k] = L / c;
+        // ref_bins: the simulator's echo bin (an integer sample index) instead of the delay
+        tau[k] = ref_bins ? 1.0 + round((L / c) * fs) : L / c;
         // exp(-j 2 pi fc tau) with the phase reduced in cycles first
         double cyc = fc * (L / c);
         cyc -= rint(cyc);
@@ -61,7 +67,7 @@ __device__ __forceinline__ double unit53(uint64_t x) { return (double)(x >> 11) 
 
 __global__ void k_echo_synth(const double* __restrict__ tau, const double2* __restrict__ carrier, int np, int ns_,
                              int nsamp, double fs, double f0, double kchirp, int nc, double sigma, uint64_t seed,
-                             double2* __restrict__ raw)
+                             int ref_bins, double2* __restrict__ raw)
 {
     const int64_t total = (int64_t)np * nsamp;
     const int half = nc / 2;
@@ -70,7 +76,18 @@ __global__ void k_echo_synth(const double* __restrict__ tau, const double2* __re
         const int p = (int)(k / nsamp), n = (int)(k % nsamp);
         double re = 0.0, im = 0.0;
         for (int s = 0; s < ns_; s++) {
-            const double t = (double)n / fs - tau[(int64_t)p * ns_ + s] + (double)half / fs;   // time inside the chirp
+            double t;                                           // time inside the chirp
+            if (ref_bins) {
+                // the simulator drops echoes whose bin falls outside the pulse (:357-359);
+                // otherwise the chirp sample index of this output in the circular convolution
+                const double bin = tau[(int64_t)p * ns_ + s];
+                if (!(bin >= 0.0 && bin < (double)nsamp)) continue;
+                int64_t m = ((int64_t)n - (int64_t)bin + half) % nsamp;
+                if (m < 0) m += nsamp;
+                t = m < nc ? (double)m / fs : -1.0;
+            } else {
+                t = (double)n / fs - tau[(int64_t)p * ns_ + s] + (double)half / fs;
+            }
             if (t >= 0.0 && t <= tmax) {
                 const double cyc = f0 * t + 0.5 * kchirp * t * t;                           // phase in cycles
                 double sn, cs;
@@ -97,20 +114,21 @@ __global__ void k_echo_synth(const double* __restrict__ tau, const double2* __re
 cudaError_t launch_echo_synth(const DemView& d, const double* tx, const double* rx, int np, const double* spos,
                               const double* samp, int nscat, double n1, double n2, int W, double c, double fc,
                               double fs, double f0, double f1, double T, int nsamp, double sigma, uint64_t seed,
-                              double* tau, double2* carrier, double2* raw, cudaStream_t st)
+                              int ref_bins, double* tau, double2* carrier, double2* raw, cudaStream_t st)
 {
     const int64_t npairs = (int64_t)np * nscat;
     int b1 = (int)((npairs + 63) / 64);
     if (b1 > 148 * 64) b1 = 148 * 64;
     if (b1 < 1) b1 = 1;
-    k_echo_paths<<<b1, 64, 0, st>>>(d, tx, rx, np, spos, samp, nscat, n1, n2, W, c, fc, tau, carrier);
+    k_echo_paths<<<b1, 64, 0, st>>>(d, tx, rx, np, spos, samp, nscat, n1, n2, W, c, fc, fs, ref_bins, tau, carrier);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     const int nc = (int)(T * fs) + 1;   // createCHIRP's sample count (src/raw_data_processing.cpp:271)
     const int64_t total = (int64_t)np * nsamp;
     int b2 = (int)((total + 255) / 256);
     if (b2 > 148 * 128) b2 = 148 * 128;
-    k_echo_synth<<<b2, 256, 0, st>>>(tau, carrier, np, nscat, nsamp, fs, f0, (f1 - f0) / T, nc, sigma, seed, raw);
+    k_echo_synth<<<b2, 256, 0, st>>>(tau, carrier, np, nscat, nsamp, fs, f0, (f1 - f0) / T, nc, sigma, seed, ref_bins,
+                                     raw);
     return cudaGetLastError();
 }
 

@@ -44,6 +44,7 @@ cudaError_t launch_upsample_store(const double2* in, int64_t n, int64_t batch, i
 cudaError_t launch_echo_synth(const DemView& d, const double* tx, const double* rx, int np, const double* spos,
                               const double* samp, int nscat, double n1, double n2, int W, double c, double fc,
                               double fs, double f0, double f1, double T, int nsamp, double sigma, uint64_t seed,
+                              int ref_bins,
                               double* tau, double2* carrier, double2* raw, cudaStream_t st);
 
 // ------------------------------- Fermat (FP64) ---------------------------------------

@@ -542,7 +542,7 @@ inline std::unique_ptr<Scene> make_scene(bsar_ctx* ctx, const bsar_scene_desc& s
 
 // Echo synthesis into a scene's raw pulses (bsar_scene_synthesize), on ctx->stream.
 inline void synthesize_samples(bsar_ctx* ctx, Scene* sc, const double* scat_pos, const double* scat_amp, int64_t n_scat,
-                               double snr_db, uint64_t seed)
+                               double snr_db, uint64_t seed, int flags = 0)
 {
     check_newton_dem(sc->dem.view);
     const int W = search_nodes(sc->dem.view, 0.0);
@@ -560,7 +560,8 @@ inline void synthesize_samples(bsar_ctx* ctx, Scene* sc, const double* scat_pos,
     const double sigma = std::isfinite(snr_db) ? std::sqrt(nc / std::pow(10.0, snr_db / 10.0)) : 0.0;
     launched(ctx, launch_echo_synth(sc->dem.view, sc->tx->as<double>(), sc->rx->as<double>(), (int)np,
                                     pos->as<double>(), amp->as<double>(), (int)n_scat, sc->n1, sc->n2, W, sc->c, sc->fc,
-                                    sc->fs, sc->f0, sc->f1, sc->T, (int)sc->ns, sigma, seed, tau->as<double>(),
+                                    sc->fs, sc->f0, sc->f1, sc->T, (int)sc->ns, sigma, seed,
+                                    (flags & BSAR_SYNTH_REFERENCE_BINS) ? 1 : 0, tau->as<double>(),
                                     car->as<double2>(), sc->samples->as<double2>(), ctx->stream),
              "echo synthesis");
     sync(ctx);   // the work buffers are released on return

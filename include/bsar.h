@@ -186,6 +186,14 @@ bsar_status bsar_scene_release(bsar_ctx* ctx, bsar_scene_id scene);
 bsar_status bsar_scene_synthesize(bsar_ctx* ctx, const bsar_scene_desc* desc, const double* scat_pos,
                                   const double* scat_amp, int64_t n_scat, double snr_db, uint64_t seed,
                                   bsar_scene_id* out);
+/* The same with flags.  BSAR_SYNTH_REFERENCE_BINS reproduces the simulator's envelope
+ * placement: each echo's chirp is centred on sample 1 + round(t*fs)
+ * (src/raw_data_processing.cpp:329) and wraps around the pulse like the simulator's
+ * circular convolution with the fftshifted chirp (:371-406); the phase stays exact. */
+enum { BSAR_SYNTH_REFERENCE_BINS = 1 };
+bsar_status bsar_scene_synthesize_ex(bsar_ctx* ctx, const bsar_scene_desc* desc, const double* scat_pos,
+                                     const double* scat_amp, int64_t n_scat, double snr_db, uint64_t seed,
+                                     int32_t flags, bsar_scene_id* out);
 
 /* Copy a scene's raw (or given compressed) pulses, Np x Ns complex, to the host. */
 bsar_status bsar_scene_read_samples(bsar_ctx* ctx, bsar_scene_id scene, double* out);

@@ -139,3 +139,32 @@ def test_gpu_echo_synthesis_noise_statistics(ctx):
     got = np.mean(np.abs(raw) ** 2)
     assert abs(got / want - 1.0) < 0.02
     assert abs(np.mean(raw)) < 0.05 * np.sqrt(want)
+
+
+def test_gpu_echo_synthesis_reference_bins(ctx):
+    """BSAR_SYNTH_REFERENCE_BINS: the simulator's echo placement (delta at sample
+    1 + round(t * fs), circular convolution with the fftshifted chirp,
+    src/raw_data_processing.cpp:292-406) restated in numpy, to 1e-9."""
+    spec = S.scaled(S.config_spec(1), n_pulses=12, n_samples=2048, n_scatterers=3, snr_db=np.inf)
+    sc = S.make_scene(spec, with_raw=False)
+    L = S.optical_paths(sc, sc.scat_pos)                       # (Np, S), FP64 Newton paths
+    N = spec.n_samples
+    chirp = S.make_chirp(spec)
+    ref = S.matched_reference(chirp, N)
+    aux = np.zeros((spec.n_pulses, N), complex)
+    for p in range(spec.n_pulses):
+        for s_ in range(len(sc.scat_amp)):
+            b = 1 + int(np.floor(L[p, s_] / 3e8 * spec.fs + 0.5))
+            if 0 <= b < N:
+                aux[p, b] += sc.scat_amp[s_] * np.exp(-2j * np.pi * spec.fc * L[p, s_] / 3e8)
+    want = np.fft.ifft(np.fft.fft(aux, axis=1) * np.fft.fft(ref)[None, :], axis=1)
+    dem = bsar.DemArrays(sc.x_vec, sc.y_vec, sc.z)
+    f0, f1 = -spec.bandwidth / 2, spec.bandwidth / 2
+    sid = ctx.scene_synthesize(dem, sc.tx, sc.rx, N, sc.scat_pos, sc.scat_amp, upsample=spec.upsample, n1=spec.n1,
+                               n2=spec.n2, c=3e8, fc=spec.fc, fs=spec.fs, chirp_f0=f0, chirp_f1=f1,
+                               chirp_T=spec.pulse_T, reference_bins=True)
+    try:
+        got = ctx.scene_read_samples(sid, spec.n_pulses, N)
+    finally:
+        ctx.scene_release(sid)
+    assert rel_l2(got, want) < 1e-9
