@@ -35,3 +35,29 @@ def test_poisson_arrivals():
     gaps = np.diff(t)
     assert abs(gaps.mean() - 1 / 50.0) < 0.02 / 50.0 * 10
     assert abs(gaps.std() / gaps.mean() - 1.0) < 0.05       # exponential: cv = 1
+
+
+def test_server_estimate_counts_request_buffers():
+    """bsar_server_estimate (host only): the bytes a request reserves grow with its
+    pulses x samples (raw + upsampled pulses), its voxels (image) and its scatterers, and
+    FP16 storage halves the upsampled part."""
+    import bsar
+
+    m = S.serve_mix(1, side=(21, 21), pulses=(128, 128), samples_log2=(11, 11), scatterers=(5, 5))
+    r = m.requests[0]
+    dem = bsar.DemArrays(r.x_vec, r.y_vec, r.z)
+
+    def est(np_=128, ns=2048, nx=21, nscat=5, precision="mixed"):
+        tx = np.repeat(r.tx[:1], np_, axis=0)
+        gx = 20 + 0.02 * np.arange(nx)
+        pos = np.repeat(r.scat_pos[:1], nscat, axis=0)
+        return bsar.Server.estimate(dem, tx, tx, gx, gx - 20, gx - 25, n_samples=ns, scat_pos=pos,
+                                    scat_amp=np.ones(nscat), precision=precision)
+
+    base = est()
+    up = 4
+    assert est(np_=256) - base == 128 * (16 * 2048 + 8 * 2048 * up + 48 + 52 + 24 * 5)
+    assert est(ns=4096) - base == 128 * (16 * 2048 + 8 * 2048 * up) + 16 * 2048
+    assert est(nx=42) - base == 16 * (42 ** 3 - 21 ** 3)
+    assert est(nscat=10) - base == 24 * 128 * 5
+    assert base - est(precision="mixed_fp16") == 4 * 128 * 2048 * up
