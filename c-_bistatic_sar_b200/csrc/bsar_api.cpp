@@ -67,10 +67,17 @@ void bsar_destroy(bsar_ctx* ctx)
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
+    clear_error(ctx);   // the destroying thread's entry; a later context may reuse the address
     delete ctx;
 }
 
-const char* bsar_last_error(const bsar_ctx* ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
+const char* bsar_last_error(const bsar_ctx* ctx)
+{
+    if (!ctx) return "null context";
+    auto& m = thread_errors();
+    auto it = m.find(ctx);
+    return it == m.end() ? "" : it->second.c_str();
+}
 
 bsar_status bsar_set_stream(bsar_ctx* ctx, void* stream)
 {

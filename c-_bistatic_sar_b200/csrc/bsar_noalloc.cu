@@ -158,10 +158,10 @@ extern "C" bsar_status bsar_backproject_mixed_noalloc(bsar_ctx* ctx, bsar_scene_
         cuda_check(cudaMemcpyAsync(&hstat, status, sizeof(int), cudaMemcpyDeviceToHost, st), "status");
         sync(ctx);
         if (hstat) fail(BSAR_ERR_TIMEOUT, "a device-side DEM tile copy did not complete within its wait limit");
-        ctx->last_error.clear();
+        clear_error(ctx);
         return BSAR_OK;
     } catch (const Error& e) {
-        ctx->last_error = e.msg;
+        set_error(ctx, e.msg);
         return e.status;
     }
 }

@@ -546,7 +546,7 @@ bsar_status bsar_server_create(bsar_ctx* ctx, const bsar_server_opts* opts, bsar
             cuda_check(cudaMemset(ctx->status->p, 0, sizeof(int)), "memset");
         }
     } catch (const Error& e) {
-        ctx->last_error = e.msg;
+        set_error(ctx, e.msg);
         return e.status;
     }
     bsar_server* raw = s.release();

@@ -80,7 +80,6 @@ struct bsar_ctx {
     uint64_t used = 0;
     uint64_t launches = 0;
     std::mutex mu;
-    std::string last_error;
     uint64_t next_scene = 1;
     std::map<uint64_t, std::unique_ptr<struct Scene>> scenes;
     std::map<std::pair<int64_t, int>, std::unique_ptr<DevBuf>> twiddles;   // (P, real bytes)
@@ -154,8 +153,20 @@ inline void launched(bsar_ctx* ctx, cudaError_t e, const char* what)
 
 inline void sync(bsar_ctx* ctx) { cuda_check(cudaStreamSynchronize(ctx->stream), "stream synchronize"); }
 
+// Last error messages, kept per calling thread and per context: bsar_last_error returns
+// the message of the calling thread's latest call on that context, so threads sharing a
+// context (the reference calls its Fermat solver from up to 12 OpenMP threads) never read
+// a string another thread is rewriting.  A successful call clears the thread's entry.
+inline std::map<const bsar_ctx*, std::string>& thread_errors()
+{
+    thread_local std::map<const bsar_ctx*, std::string> m;
+    return m;
+}
+inline void set_error(const bsar_ctx* ctx, const std::string& msg) { thread_errors()[ctx] = msg; }
+inline void clear_error(const bsar_ctx* ctx) { thread_errors().erase(ctx); }
+
 // Runs an entry point's body with the context locked and its device current, turning
-// errors into a status and the context's last error.
+// errors into a status and the calling thread's last error.
 template <typename F> inline bsar_status guarded(bsar_ctx* ctx, F&& f)
 {
     if (!ctx) return BSAR_ERR_INVALID_ARG;
@@ -163,13 +174,13 @@ template <typename F> inline bsar_status guarded(bsar_ctx* ctx, F&& f)
     try {
         cuda_check(cudaSetDevice(ctx->device), "cudaSetDevice");
         f();
-        ctx->last_error.clear();
+        clear_error(ctx);
         return BSAR_OK;
     } catch (const Error& e) {
-        ctx->last_error = e.msg;
+        set_error(ctx, e.msg);
         return e.status;
     } catch (const std::bad_alloc&) {
-        ctx->last_error = "host allocation failed";
+        set_error(ctx, "host allocation failed");
         return BSAR_ERR_OOM_BUDGET;
     }
 }

@@ -14,7 +14,9 @@
  *   - Host buffers are caller-owned and only read / written during the call; device
  *     memory is owned by the context.  Every call is synchronous unless its name ends
  *     in _device.
- *   - Every entry point returns a bsar_status; bsar_last_error() gives the message.
+ *   - Every entry point returns a bsar_status; bsar_last_error(ctx) gives the message of
+ *     the calling thread's latest call on ctx (empty after a success), so threads that
+ *     share a context each read their own failure.
  *     There is no CPU fallback: without a usable CUDA device bsar_create fails.
  *   - A context is internally locked; calls from several threads are serialised.
  */
