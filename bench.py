@@ -74,6 +74,7 @@ class ClockSampler:
         self.rows = []
         self.proc = None
         self.thread = None
+        self.first = threading.Event()
 
     def __enter__(self):
         try:
@@ -82,6 +83,9 @@ class ClockSampler:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # nvidia-smi's start-up (NVML initialisation) is kept out of the caller's
+            # timed region: wait for the first sample
+            self.first.wait(timeout=10)
         except OSError:
             self.proc = None
         return self
@@ -89,6 +93,8 @@ class ClockSampler:
     def _read(self):
         for line in self.proc.stdout:
             self.rows.append([c.strip() for c in line.split(",")])
+            self.first.set()
+        self.first.set()
 
     def __exit__(self, *a):
         if self.proc:
@@ -139,6 +145,20 @@ def make_workload(cfg: int, rank: int, nz: int = 0):
         # weak scaling: rank r images the next z-slab of the same size
         sc.gz = sc.gz - rank * spec.nz * spec.dz
     return sc
+
+
+def time_compress(ctx, torch, stream, sid, precision, reps=10):
+    """Median device time of one scene compression (pulse compression + x4 upsampling into
+    the form's storage), `reps` launches back to back after one untimed launch.  The raw
+    pulses and the upsampled storage are larger than L2, so no flush is needed."""
+    ctx.scene_compress(sid, precision)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+    for a, b in ev:
+        a.record(stream)
+        ctx.scene_compress(sid, precision)
+        b.record(stream)
+    torch.cuda.synchronize()
+    return statistics.median(a.elapsed_time(b) for a, b in ev)
 
 
 def time_device(ctx, torch, stream, sid, sc, precision, solver, legs, steps, warmup, gx=None, gy=None, gz=None):
@@ -554,12 +574,15 @@ def main():
                 "fp32_flops_per_voxel_pulse": fp32_flops_per_voxel_pulse(W), "node_scan_half_width": W}
 
     # pulse compression (K1): HBM roofline on raw in + upsampled complex64 out
-    pc_ms = max_over_ranks(statistics.mean(time_device.pc_ms))
+    # one compression as its own launches (inside the step it sits between back-projection
+    # launches of ~0.6 s, where single-launch event times are noisy)
+    pc_ms = max_over_ranks(time_compress(ctx, torch, stream, sid, "mixed"))
     ns = sp.n_samples
     pc_bytes = sp.n_pulses * (16 * ns + 8 * ns * sp.upsample)
     pc_gbs = pc_bytes / (pc_ms / 1e3) / 1e9
     roofline["pulse_compression"] = {
-        "kernel": "k_pulse_compress<float>", "ms": pc_ms, "samples_per_s": sp.n_pulses * ns / (pc_ms / 1e3),
+        "kernel": (f"k_pulse_compress_rf<{int(math.log2(ns))}>" if 4096 <= ns <= 16384 else "k_pulse_compress<float>"),
+        "ms": pc_ms, "samples_per_s": sp.n_pulses * ns / (pc_ms / 1e3),
         "bytes": pc_bytes, "achieved_gbs": pc_gbs, "peak_gbs": peaks.get("hbm_gbs"), "frac": pc_gbs / peaks.get("hbm_gbs", 1),
         "flops": sp.n_pulses * 2 * (10 * ns * math.log2(ns) + 6 * ns)}
     roofline["fermat"] = {"solves_per_s": 2 * vp / (bp_avg_ms / 1e3),

@@ -46,6 +46,23 @@ bsar_status bsar_create(bsar_ctx** out, const bsar_opts* opts)
         return BSAR_ERR_CUDA;
     }
     ctx->own_stream = true;
+    // the context's device buffers come from its own stream-ordered pool, which keeps
+    // freed blocks for the next call: a cudaMalloc / cudaFree per call costs a
+    // device-wide synchronisation each and, now and then, hundreds of milliseconds
+    {
+        cudaMemPoolProps pp = {};
+        pp.allocType = cudaMemAllocationTypePinned;
+        pp.location.type = cudaMemLocationTypeDevice;
+        pp.location.id = dev;
+        uint64_t keep = ~0ull;
+        if (cudaMemPoolCreate(&ctx->pool, &pp) != cudaSuccess ||
+            cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess) {
+            if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
+            ctx->pool = nullptr;
+            cudaGetLastError();
+        }
+        ctx->use_pool = ctx->pool != nullptr;
+    }
     size_t fr = 0, tot = 0;
     cudaMemGetInfo(&fr, &tot);
     ctx->budget = (opts && opts->hbm_budget_bytes) ? opts->hbm_budget_bytes : (uint64_t)(0.9 * (double)fr);

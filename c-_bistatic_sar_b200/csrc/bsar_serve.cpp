@@ -124,16 +124,17 @@ template <typename F> void with_ctx(bsar_server* s, cudaStream_t st, bool pooled
     std::lock_guard<std::mutex> lk(s->ctx->mu);
     cudaStream_t saved = s->ctx->stream;
     s->ctx->stream = st;
+    const bool saved_pool = s->ctx->use_pool;
     s->ctx->use_pool = pooled;
     try {
         f();
     } catch (...) {
         s->ctx->stream = saved;
-        s->ctx->use_pool = false;
+        s->ctx->use_pool = saved_pool;
         throw;
     }
     s->ctx->stream = saved;
-    s->ctx->use_pool = false;
+    s->ctx->use_pool = saved_pool;
 }
 
 void finish(bsar_server* s, Req* r, bsar_status st, const std::string& err)
@@ -524,6 +525,15 @@ bsar_status bsar_server_create(bsar_ctx* ctx, const bsar_server_opts* opts, bsar
             uint64_t keep = ~0ull;     // keep freed blocks for the next admission
             cuda_check(cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep), "pool attribute");
         }
+        // the batch records and the status word are used from the batch streams: plain
+        // device allocations, not stream-ordered ones on the context's stream
+        const bool saved_pool = ctx->use_pool;
+        ctx->use_pool = false;
+        struct RestorePool {
+            bsar_ctx* c;
+            bool v;
+            ~RestorePool() { c->use_pool = v; }
+        } restore_pool{ctx, saved_pool};
         // admission outranks the batches: its kernels take the SM slots the batch CTAs
         // free before the queued batch does, so a request is ready for the next batch
         int least = 0, greatest = 0;

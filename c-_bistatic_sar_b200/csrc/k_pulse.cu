@@ -205,6 +205,43 @@ __device__ __forceinline__ void hermite_store32(Load ld, int64_t n, int factor, 
                                       (float)(t3 - 2 * t2 + t), (float)(t3 - t2));
     }
     __syncthreads();
+    // x4 (the imager's factor) into 16-byte aligned storage: the interval's four outputs
+    // leave as two 16-byte stores (complex64) or one (FP16 complex), same values
+    const void* out_base = out_kind == 1 ? (const void*)out32 : (const void*)out16;
+    if (factor == 4 && (reinterpret_cast<uintptr_t>(out_base) & 15) == 0) {
+        const float4 ws[4] = {wt[0], wt[1], wt[2], wt[3]};
+        for (int64_t iv = threadIdx.x; iv < n; iv += blockDim.x) {
+            float2 o[4];
+            if (iv >= n - 1) {
+                o[0] = o[1] = o[2] = o[3] = ld(n - 1);
+            } else {
+                const float2 pm1 = ld(iv > 0 ? iv - 1 : 0), p0 = ld(iv), p1 = ld(iv + 1),
+                             p2 = ld(iv + 2 < n ? iv + 2 : n - 1);
+                const float dpx = iv > 0 ? p0.x - pm1.x : 0.f, dpy = iv > 0 ? p0.y - pm1.y : 0.f;
+                const float dnx = iv < n - 2 ? p2.x - p1.x : 0.f, dny = iv < n - 2 ? p2.y - p1.y : 0.f;
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const float4 w = ws[k];
+                    o[k].x = fmaf(w.x, p0.x, fmaf(w.y, p1.x, fmaf(w.z, dpx, w.w * dnx)));
+                    o[k].y = fmaf(w.x, p0.y, fmaf(w.y, p1.y, fmaf(w.z, dpy, w.w * dny)));
+                }
+            }
+            if (out_kind == 1) {
+                float4* d = reinterpret_cast<float4*>(out32 + iv * 4);
+                d[0] = make_float4(o[0].x, o[0].y, o[1].x, o[1].y);
+                d[1] = make_float4(o[2].x, o[2].y, o[3].x, o[3].y);
+            } else {
+                unsigned u[4];
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const __half2 h = __floats2half2_rn(o[k].x * inv_scale, o[k].y * inv_scale);
+                    u[k] = *reinterpret_cast<const unsigned*>(&h);
+                }
+                *reinterpret_cast<uint4*>(out16 + iv * 4) = make_uint4(u[0], u[1], u[2], u[3]);
+            }
+        }
+        return;
+    }
     for (int64_t iv = threadIdx.x; iv < n; iv += blockDim.x) {
         const int64_t o0 = iv * factor;
         if (iv >= n - 1) {
@@ -327,6 +364,235 @@ __global__ void k_pulse_compress(const double2* __restrict__ in, int ns, int P, 
         else
             out16[dst] = __floats2half2_rn((float)re * inv_scale, (float)im * inv_scale);
     }
+}
+
+// ---------------------------------------------------------------------------------
+// FP32 pulse compression with the transforms held in registers, P = 2^L, L = 12..14.
+//
+// P/16 threads, 16 elements each.  A pass loads one group of 16 elements per thread,
+// runs four radix-2 stages on it in registers and stores it back; the stages of a
+// transform fall into three passes (spans P/2..P/16, P/32..P/256, then the rest), and
+// the middle pass of the pair of transforms does the forward transform's last stages,
+// the matched-filter multiply and the inverse transform's first stages together:
+//   pass 1   elements t + (P/16) m      from global memory (the raw pulse)
+//   pass 2   elements b (P/16) + o + B m,         B = 16 TB
+//   pass 3   elements c B + s + TB m,             TB = 2^(L-12) threads share a block
+// Stages whose span is below TB pair elements of neighbouring lanes and run through warp
+// shuffles.  Every butterfly, twiddle and operation order is that of fft_dif / fft_dit,
+// so the result is the same, bit for bit, as k_pulse_compress<float>; only the grouping
+// of stages into shared-memory round trips changes (5 instead of 16).
+//
+// Shared memory holds the P elements unpadded, at x[swz(e)]: the XOR swizzle permutes
+// elements inside blocks of 16 TB, keyed by the block index, so that the 16 lanes of a
+// half-warp hit 16 different bank pairs in every pass (passes 1 and 2 read consecutive
+// elements of one block; pass 3 reads one element of each of several blocks).
+// ---------------------------------------------------------------------------------
+template <int L> __device__ __forceinline__ int swz(int e)
+{
+    constexpr int lt = L - 12;
+    return e ^ (((e >> (4 + lt)) & (15 >> lt)) << lt);
+}
+
+// The opaque copy of `base` makes each call compute its 16 addresses afresh, instead of
+// the compiler keeping a pass's addresses live until the inverse pass reuses them.
+template <int L, int STRIDE>
+__device__ __forceinline__ void rf_load(const float2* x, float2 (&v)[16], int base)
+{
+    asm volatile("" : "+r"(base));
+#pragma unroll
+    for (int m = 0; m < 16; m++) v[m] = x[swz<L>(base + STRIDE * m)];
+}
+
+template <int L, int STRIDE>
+__device__ __forceinline__ void rf_store(float2* x, const float2 (&v)[16], int base)
+{
+    asm volatile("" : "+r"(base));
+#pragma unroll
+    for (int m = 0; m < 16; m++) x[swz<L>(base + STRIDE * m)] = v[m];
+}
+
+// Four DIF stages (spans 8, 4, 2, 1 x STRIDE) on elements base + STRIDE m; r = base mod
+// STRIDE, so element e of a pair (e, e + h) has twiddle index (e mod h) P / (2h) =
+// (r + STRIDE (m mod d)) P / (2 STRIDE d).
+template <int L, int STRIDE>
+__device__ __forceinline__ void rf_dif4(float2 (&v)[16], int r, const float2* __restrict__ tw)
+{
+    constexpr int P = 1 << L;
+#pragma unroll
+    for (int d = 8; d >= 1; d >>= 1) {
+        const int tstep = P / (2 * STRIDE * d);
+        asm volatile("" ::: "memory");     // keep later stages' twiddle loads after this stage
+#pragma unroll
+        for (int m = 0; m < 16; m++) {
+            if (m & d) continue;
+            const float2 a = v[m], b = v[m + d];
+            v[m] = cadd(a, b);
+            v[m + d] = cmul(csub(a, b), __ldg(tw + (r + STRIDE * (m & (d - 1))) * tstep));
+        }
+    }
+}
+
+// Four DIT stages (spans 1, 2, 4, 8 x STRIDE), twiddles as in rf_dif4.
+template <int L, int STRIDE>
+__device__ __forceinline__ void rf_dit4(float2 (&v)[16], int r, const float2* __restrict__ tw)
+{
+    constexpr int P = 1 << L;
+#pragma unroll
+    for (int d = 1; d <= 8; d <<= 1) {
+        const int tstep = P / (2 * STRIDE * d);
+        asm volatile("" ::: "memory");
+#pragma unroll
+        for (int m = 0; m < 16; m++) {
+            if (m & d) continue;
+            const float2 a = v[m], t = cmul(v[m + d], __ldg(tw + (r + STRIDE * (m & (d - 1))) * tstep));
+            v[m] = cadd(a, t);
+            v[m + d] = csub(a, t);
+        }
+    }
+}
+
+__device__ __forceinline__ float2 shfl_xor2(float2 a, int s)
+{
+    a.x = __shfl_xor_sync(0xffffffffu, a.x, s);
+    a.y = __shfl_xor_sync(0xffffffffu, a.y, s);
+    return a;
+}
+
+// DIF stage of span s < TB across lanes (lane ^ s holds the partner): the lane whose
+// element has bit s clear keeps a + b, its partner (a - b) w, w = tw[(sub mod s) P/(2s)].
+template <int L>
+__device__ __forceinline__ void rf_dif_lanes(float2 (&v)[16], int sub, int s, const float2* __restrict__ tw)
+{
+    constexpr int P = 1 << L;
+    const bool hi = sub & s;
+    const float2 w = __ldg(tw + (sub & (s - 1)) * (P / (2 * s)));
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+        const float2 o = shfl_xor2(v[m], s);
+        v[m] = hi ? cmul(csub(o, v[m]), w) : cadd(v[m], o);
+    }
+}
+
+// DIT stage of span s < TB across lanes: t = b w, a + t to the lane holding a, a - t
+// to the lane holding b.
+template <int L>
+__device__ __forceinline__ void rf_dit_lanes(float2 (&v)[16], int sub, int s, const float2* __restrict__ tw)
+{
+    constexpr int P = 1 << L;
+    const bool hi = sub & s;
+    const float2 w = __ldg(tw + (sub & (s - 1)) * (P / (2 * s)));
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+        const float2 o = shfl_xor2(v[m], s);
+        v[m] = hi ? csub(o, cmul(v[m], w)) : cadd(v[m], cmul(o, w));
+    }
+}
+
+// CTAs per SM the register budget is sized for: two (64 registers a thread at 512 threads,
+// 128 at 256); one at 1024 threads.
+template <int L> struct RfOcc { static constexpr int v = L == 14 ? 1 : 2; };
+
+template <int L>
+__global__ void __launch_bounds__((1 << L) / 16, RfOcc<L>::v)
+    k_pulse_compress_rf(const double2* __restrict__ in, int ns, const float2* __restrict__ tw,
+                        const float2* __restrict__ spec, int n_keep, int factor, int out_kind,
+                        double2* __restrict__ out64, float2* __restrict__ out32, __half2* __restrict__ out16,
+                        float* __restrict__ scale16)
+{
+    constexpr int P = 1 << L, T = P / 16, TB = 1 << (L - 12), B = 16 * TB;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2* x = reinterpret_cast<float2*>(smem_raw);
+    __shared__ float red[32];
+    const int t = threadIdx.x;
+    const int64_t p = blockIdx.x;
+    const double2* __restrict__ src = in + p * (int64_t)ns;
+    float2 v[16];
+    // pass 1: the raw pulse (zero-padded to P) straight into registers, eight FP64 loads
+    // in flight at a time
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+#pragma unroll
+        for (int m = 8 * h; m < 8 * h + 8; m++) {
+            const int i = t + T * m;
+            const double2 d = i < ns ? __ldg(src + i) : make_double2(0.0, 0.0);
+            v[m] = make_float2((float)d.x, (float)d.y);
+        }
+        asm volatile("" ::: "memory");
+    }
+    rf_dif4<L, T>(v, t, tw);
+    rf_store<L, T>(x, v, t);
+    __syncthreads();
+    // pass 2
+    const int o2 = t % B, b2 = (t / B) * T + o2;
+    rf_load<L, B>(x, v, b2);
+    rf_dif4<L, B>(v, o2, tw);
+    rf_store<L, B>(x, v, b2);
+    __syncthreads();
+    // pass 3: last forward stages, matched filter, first inverse stages
+    const int sub = t % TB, b3 = (t / TB) * B + sub;
+    rf_load<L, TB>(x, v, b3);
+    rf_dif4<L, TB>(v, sub, tw);
+#pragma unroll
+    for (int s = TB / 2; s >= 1; s >>= 1) rf_dif_lanes<L>(v, sub, s, tw);
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        asm volatile("" ::: "memory");
+#pragma unroll
+        for (int m = 8 * h; m < 8 * h + 8; m++) v[m] = cmul(cconj(v[m]), __ldg(spec + b3 + TB * m));
+    }
+#pragma unroll
+    for (int s = 1; s < TB; s <<= 1) rf_dit_lanes<L>(v, sub, s, tw);
+    rf_dit4<L, TB>(v, sub, tw);
+    rf_store<L, TB>(x, v, b3);
+    __syncthreads();
+    // passes 2 and 1 of the inverse transform, then conj / P
+    rf_load<L, B>(x, v, b2);
+    rf_dit4<L, B>(v, o2, tw);
+    rf_store<L, B>(x, v, b2);
+    __syncthreads();
+    rf_load<L, T>(x, v, t);
+    rf_dit4<L, T>(v, t, tw);
+    const float invP = 1.0f / (float)P;
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+        v[m].x = v[m].x * invP;
+        v[m].y = -v[m].y * invP;
+    }
+    rf_store<L, T>(x, v, t);
+    __syncthreads();
+    auto ld = [&](int64_t i) { return x[swz<L>((int)i)]; };
+    if (factor <= 0) {
+        double2* dst = out64 + p * (int64_t)n_keep;
+        for (int i = t; i < n_keep; i += T) {
+            const float2 c = ld(i);
+            dst[i] = make_double2((double)c.x, (double)c.y);
+        }
+        return;
+    }
+    const int64_t n = n_keep, nout = n * factor;
+    float scale = 1.0f;
+    if (out_kind == 2) {
+        float mx = 0.0f;
+        for (int i = t; i < n; i += T) {
+            const float2 c = ld(i);
+            mx = fmaxf(mx, fmaxf(fabsf(c.x), fabsf(c.y)));
+        }
+        for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        if ((t & 31) == 0) red[t >> 5] = mx;
+        __syncthreads();
+        if (t < 32) {
+            mx = (t < (T >> 5)) ? red[t] : 0.0f;
+            for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+            if (t == 0) red[0] = mx;
+        }
+        __syncthreads();
+        mx = red[0];
+        // the Hermite overshoot stays well inside 2x the sample maximum
+        scale = (mx > 0.0f) ? mx / 16384.0f : 1.0f;
+        if (t == 0) scale16[p] = scale;
+    }
+    hermite_store32(ld, n, factor, out_kind, 1.0f / scale, out32 ? out32 + p * nout : nullptr,
+                    out16 ? out16 + p * nout : nullptr);
 }
 
 // Upsampling of already-compressed pulses into the mixed forms' storage (complex64, or
@@ -706,8 +972,28 @@ cudaError_t launch_ref_spectrum(const double2* ref, int nref, int P, int logP, c
     return cudaGetLastError();
 }
 
+template <int L> static cudaError_t launch_pulse_rf(const PulseArgs& a, cudaStream_t st)
+{
+    const size_t sm = (size_t)(1 << L) * sizeof(float2);
+    cudaFuncSetAttribute(k_pulse_compress_rf<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    // 60 % of the unified memory as shared memory holds two CTAs' pulses; the rest stays
+    // L1 for the twiddles, the reference spectrum and register spills
+    cudaFuncSetAttribute(k_pulse_compress_rf<L>, cudaFuncAttributePreferredSharedMemoryCarveout, 60);
+    k_pulse_compress_rf<L><<<(unsigned)a.batch, (1 << L) / 16, sm, st>>>(
+        a.in, a.ns, (const float2*)a.tw, (const float2*)a.spec, a.n_keep, a.factor, a.out_kind, a.out64, a.out32,
+        a.out16, a.scale16);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_pulse_compress(const PulseArgs& a, cudaStream_t st)
 {
+    // FP32 transforms of 4096..16384 points into FP32 storage (or none): registers
+    if (a.real_bytes == 4 && (a.factor <= 0 || a.out_kind != 0) && a.logP >= 12 && a.logP <= 14 &&
+        a.P == (1 << a.logP)) {
+        if (a.logP == 12) return launch_pulse_rf<12>(a, st);
+        if (a.logP == 13) return launch_pulse_rf<13>(a, st);
+        return launch_pulse_rf<14>(a, st);
+    }
     const int C = cluster_size(a.P, a.real_bytes);
     if (C > 1) {
         const int logM = a.logP - __builtin_ctz(C);

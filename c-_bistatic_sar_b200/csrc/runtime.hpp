@@ -90,9 +90,11 @@ struct bsar_ctx {
     std::unique_ptr<DevBuf> status;
     // one-request mixed launch: request record and work counter
     std::unique_ptr<DevBuf> mixed_req, mixed_counter;
-    // stream-ordered pool: while `use_pool` is set, buffers come from it (allocation and
-    // release on the current stream, without the device-wide synchronisation of
-    // cudaMalloc / cudaFree); the server's admission path runs this way next to batches
+    // stream-ordered pool: while `use_pool` is set (the default), buffers come from it,
+    // allocated and released on the context's current stream without the device-wide
+    // synchronisation of cudaMalloc / cudaFree; freed blocks stay in the pool until
+    // bsar_destroy.  Buffers that other streams use (the server's batch records) are
+    // taken with `use_pool` cleared.
     cudaMemPool_t pool = nullptr;
     bool use_pool = false;
 };
@@ -620,8 +622,19 @@ inline void set_anchors(bsar_ctx* ctx, Scene* s, const bsar_grid* g, BpArgs& a)
 inline void ensure_mixed_buffers(bsar_ctx* ctx)
 {
     if (!ctx->status) {
-        ctx->status = dev_alloc(ctx, sizeof(int));
+        // the status word is shared with the server's batch streams: a plain allocation,
+        // cleared before any stream can use it
+        const bool pooled = ctx->use_pool;
+        ctx->use_pool = false;
+        try {
+            ctx->status = dev_alloc(ctx, sizeof(int));
+        } catch (...) {
+            ctx->use_pool = pooled;
+            throw;
+        }
+        ctx->use_pool = pooled;
         cuda_check(cudaMemsetAsync(ctx->status->p, 0, sizeof(int), ctx->stream), "memset");
+        sync(ctx);
     }
     if (!ctx->mixed_req) ctx->mixed_req = dev_alloc(ctx, sizeof(MixedReq));
     if (!ctx->mixed_counter) ctx->mixed_counter = dev_alloc(ctx, sizeof(int));

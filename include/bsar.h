@@ -12,7 +12,9 @@
  *     pairs; point arrays are n x 3 row-major (x, y, z); pulses are pulse-major
  *     (sample s of pulse p at [p * n + s]).
  *   - Host buffers are caller-owned and only read / written during the call; device
- *     memory is owned by the context.  Every call is synchronous unless its name ends
+ *     memory is owned by the context.  The context takes it from its own stream-ordered
+ *     pool (cudaMallocFromPoolAsync on the context's stream), which keeps freed blocks
+ *     for later calls until bsar_destroy; bsar_bytes_in_use counts the live buffers.  Every call is synchronous unless its name ends
  *     in _device.
  *   - Every entry point returns a bsar_status; bsar_last_error(ctx) gives the message of
  *     the calling thread's latest call on ctx (empty after a success), so threads that

@@ -97,6 +97,25 @@ def test_scene_compress_long_pulses(ctx, oracle):
     assert rel_l2(got["mixed_fp16"], o) < 2e-3
 
 
+@pytest.mark.parametrize("ns", [4096, 8192])
+def test_scene_compress_fp32_register_transforms(ctx, oracle, ns):
+    """FP32 pulses of 4096 and 8192 samples (the register-resident transforms with the
+    16-byte x4 epilogue) into complex64 and FP16 storage, against the FP64 oracle."""
+    spec = S.scaled(S.config_spec(2), n_pulses=5, n_samples=ns, n_scatterers=8)
+    sc = S.make_scene(spec)
+    o = oracle.spline_upsample(oracle.fft_correlate(sc.raw, sc.reference), 4)
+    sid = bsar.upload_scene(ctx, sc)
+    try:
+        m32 = ctx.scene_read_stored(sid, spec.n_pulses, ns * 4, "mixed")
+        m16 = ctx.scene_read_stored(sid, spec.n_pulses, ns * 4, "mixed_fp16")
+    finally:
+        ctx.scene_release(sid)
+    assert rel_l2(m32, o) < 1e-5
+    assert rel_l2(m16, o) < 2e-3
+    # the last input interval repeats the last sample (splineInterpolation's clamp)
+    assert np.array_equal(m32[:, -4:], np.repeat(m32[:, -4:-3], 4, axis=1))
+
+
 def test_matched_filter_peak_at_lag_zero(ctx, sc):
     out = ctx.fft_correlate(sc.reference[None, :], sc.reference)
     assert int(np.argmax(np.abs(out[0]))) == 0
