@@ -11,6 +11,10 @@
 // src/interpolation.cpp:4-51 runs as the epilogue, reading neighbours from shared
 // memory and writing the upsampled pulse in the requested storage type.
 //
+// FP32 pulses of 4096..16384 samples into FP32 storage take k_pulse_compress_rf instead:
+// the same butterflies with the transforms held in registers, 16 elements per thread, and
+// 5 shared-memory exchanges per pulse instead of one per pair of stages.
+//
 // Pulses longer than one CTA's shared memory holds (FP64 above 8192, FP32 above 16384
 // samples) run on a thread-block cluster of C = 2..8 CTAs: CTA r holds elements
 // [r*M, (r+1)*M), M = P/C.  The radix-2 stages whose span reaches M pair elements of two
