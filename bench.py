@@ -347,6 +347,14 @@ def serve_leg(ctx, torch, n_requests: int, burst: int, fp64_sample: int, load: f
     return out
 
 
+def workload_name(sp) -> str:
+    """The workload a bench line is quoted on (both arms name it the same way)."""
+    return (f"{sp.name}: {sp.nx}x{sp.ny}x{sp.nz} voxels at {sp.dxy} m, {sp.n_pulses} pulses, "
+            f"{sp.n_samples}->{sp.n_samples * sp.upsample} fast-time samples, "
+            f"{sp.dem_n}^2 fBm DEM ({sp.dem_d} m, sigma {sp.dem_sigma} m), eps_r {sp.eps_r}, "
+            f"{sp.n_scatterers} scatterers, {sp.snr_db} dB")
+
+
 def run_reference(args):
     """--impl reference: the reference's CPU implementation on the box's host cores."""
     rank = int(os.environ.get("RANK", "0"))
@@ -371,9 +379,8 @@ def run_reference(args):
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": sp.voxel_pulses / value * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded; no dataset)",
-            "config": {"workload": f"{sp.name}: {sp.nx}x{sp.ny}x{sp.nz} voxels, {sp.n_pulses} pulses, "
-                                   f"{sp.n_samples}->{sp.n_samples * sp.upsample} samples, "
-                                   f"{sp.dem_n}^2 fBm DEM", "form": "reference CPU (grid search, mean legs)"},
+            "config": {"workload": workload_name(sp), "form": "reference CPU (grid search, mean legs)",
+                       "parallelism": f"rank 0 only, {details['cores']} host threads"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": details["cores"], "kind": details["kind"],
                              "sample": details["sample"]},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -620,10 +627,7 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+f64 (mixed)", "data": "synthetic (seeded; no dataset)",
-            "config": {"workload": f"{sp.name}: {sp.nx}x{sp.ny}x{sp.nz} voxels at {sp.dxy} m, {sp.n_pulses} pulses, "
-                                   f"{sp.n_samples}->{sp.n_samples * sp.upsample} fast-time samples, "
-                                   f"{sp.dem_n}^2 fBm DEM ({sp.dem_d} m, sigma {sp.dem_sigma} m), eps_r {sp.eps_r}, "
-                                   f"{sp.n_scatterers} scatterers, {sp.snr_db} dB",
+            "config": {"workload": workload_name(sp),
                        "form": "mixed (Newton Fermat FP32 + FP64 final step, complex64 samples, Kahan FP32 sums)",
                        "per_gpu": "one z-slab of the full grid size per rank",
                        "l2": "inputs larger than L2 (upsampled complex64 pulses "
