@@ -97,23 +97,24 @@ def test_scene_compress_long_pulses(ctx, oracle):
     assert rel_l2(got["mixed_fp16"], o) < 2e-3
 
 
-@pytest.mark.parametrize("ns", [4096, 8192])
-def test_scene_compress_fp32_register_transforms(ctx, oracle, ns):
-    """FP32 pulses of 4096 and 8192 samples (the register-resident transforms with the
-    16-byte x4 epilogue) into complex64 and FP16 storage, against the FP64 oracle."""
-    spec = S.scaled(S.config_spec(2), n_pulses=5, n_samples=ns, n_scatterers=8)
+@pytest.mark.parametrize("ns,factor", [(4096, 4), (8192, 4), (4096, 2), (8192, 8)])
+def test_scene_compress_fp32_register_transforms(ctx, oracle, ns, factor):
+    """FP32 pulses of 4096 and 8192 samples (the register-resident transforms; x4 with the
+    16-byte epilogue stores, other factors with one store per output) into complex64 and
+    FP16 storage, against the FP64 oracle."""
+    spec = S.scaled(S.config_spec(2), n_pulses=5, n_samples=ns, n_scatterers=8, upsample=factor)
     sc = S.make_scene(spec)
-    o = oracle.spline_upsample(oracle.fft_correlate(sc.raw, sc.reference), 4)
+    o = oracle.spline_upsample(oracle.fft_correlate(sc.raw, sc.reference), factor)
     sid = bsar.upload_scene(ctx, sc)
     try:
-        m32 = ctx.scene_read_stored(sid, spec.n_pulses, ns * 4, "mixed")
-        m16 = ctx.scene_read_stored(sid, spec.n_pulses, ns * 4, "mixed_fp16")
+        m32 = ctx.scene_read_stored(sid, spec.n_pulses, ns * factor, "mixed")
+        m16 = ctx.scene_read_stored(sid, spec.n_pulses, ns * factor, "mixed_fp16")
     finally:
         ctx.scene_release(sid)
     assert rel_l2(m32, o) < 1e-5
     assert rel_l2(m16, o) < 2e-3
     # the last input interval repeats the last sample (splineInterpolation's clamp)
-    assert np.array_equal(m32[:, -4:], np.repeat(m32[:, -4:-3], 4, axis=1))
+    assert np.array_equal(m32[:, -factor:], np.repeat(m32[:, -factor:-factor + 1], factor, axis=1))
 
 
 def test_matched_filter_peak_at_lag_zero(ctx, sc):
