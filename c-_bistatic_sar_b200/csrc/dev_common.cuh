@@ -93,19 +93,33 @@ __device__ __forceinline__ double grid_optical(double px, double py, double pz, 
 
 // One level of the reference's grid search (:509-551) with a G x G grid.  The y-axis
 // lookups of the G columns do not depend on the row, so they are made once per level.
-template <int G>
+// Column tables of one search level in shared memory, [column][thread] (consecutive
+// lanes, consecutive words): the G column positions and y-axis lookups stay out of the
+// registers.  TPB is the largest block the calling kernel launches with.
+template <int TPB> struct GridCols {
+    double py[15][TPB];
+    double w[15][TPB];
+    int2 ii[15][TPB];
+};
+
+template <int G, int TPB>
 __device__ __forceinline__ void grid_level(const DemView& d, double x1, double y1, double z1,
                                            double x2, double y2, double z2, double n1, double n2,
-                                           double R, double& bestX, double& bestY, double& minOP)
+                                           double R, double& bestX, double& bestY, double& minOP,
+                                           GridCols<TPB>* cols)
 {
     const double minX = bestX - R, maxX = bestX + R;
     const double minY = bestY - R, maxY = bestY + R;
-    double py[G];
-    AxisLookup ay[G];
+    const int t = threadIdx.x;
 #pragma unroll
     for (int j = 0; j < G; j++) {
-        py[j] = minY + j * (maxY - minY) / (G - 1);
-        if (!d.empty) ay[j] = axis_lookup(d.yv, d.ny, py[j], d.asc_y);
+        const double py = minY + j * (maxY - minY) / (G - 1);
+        cols->py[j][t] = py;
+        if (!d.empty) {
+            const AxisLookup a = axis_lookup(d.yv, d.ny, py, d.asc_y);
+            cols->w[j][t] = a.w;
+            cols->ii[j][t] = make_int2(a.i0, a.i1);
+        }
     }
     for (int i = 0; i < G; i++) {
         double px = minX + i * (maxX - minX) / (G - 1);
@@ -113,32 +127,40 @@ __device__ __forceinline__ void grid_level(const DemView& d, double x1, double y
         if (!d.empty) ax = axis_lookup(d.xv, d.nx, px, d.asc_x);
 #pragma unroll
         for (int j = 0; j < G; j++) {
-            double pz = d.empty ? 0.0 : dem_combine(d, ax, ay[j]);
-            double op = grid_optical(px, py[j], pz, x1, y1, z1, x2, y2, z2, n1, n2);
+            const double py = cols->py[j][t];
+            double pz = 0.0;
+            if (!d.empty) {
+                const int2 ii = cols->ii[j][t];
+                const AxisLookup ay{ii.x, ii.y, cols->w[j][t]};
+                pz = dem_combine(d, ax, ay);
+            }
+            double op = grid_optical(px, py, pz, x1, y1, z1, x2, y2, z2, n1, n2);
             if (op < minOP) {
                 minOP = op;
                 bestX = px;
-                bestY = py[j];
+                bestY = py;
             }
         }
     }
 }
 
 // calculateRefractionPoint, src/raw_data_processing.cpp:455-572.
+template <int TPB>
 __device__ __forceinline__ void refraction_grid(const DemView& d, double x1, double y1, double z1,
                                                 double x2, double y2, double z2, double n1,
                                                 double n2, double out[3])
 {
+    __shared__ GridCols<TPB> cols;
     double bestX = (x1 + x2) / 2.0;
     double bestY = (y1 + y2) / 2.0;
     double dd = sqrt((x2 - x1) * (x2 - x1) + (y2 - y1) * (y2 - y1));
     double R = std_max(dd, 500.0);
     double minOP = 1e9;
-    grid_level<15>(d, x1, y1, z1, x2, y2, z2, n1, n2, R, bestX, bestY, minOP);
+    grid_level<15, TPB>(d, x1, y1, z1, x2, y2, z2, n1, n2, R, bestX, bestY, minOP, &cols);
     R /= 5.0;
 #pragma unroll 1
     for (int level = 1; level < 5; level++) {
-        grid_level<11>(d, x1, y1, z1, x2, y2, z2, n1, n2, R, bestX, bestY, minOP);
+        grid_level<11, TPB>(d, x1, y1, z1, x2, y2, z2, n1, n2, R, bestX, bestY, minOP, &cols);
         R /= 3.0;
     }
     out[0] = bestX;
@@ -342,12 +364,14 @@ __device__ __forceinline__ void refraction_newton(const DemView& d, const double
 }
 
 // Dispatch on the solver (0 = grid, 1 = Newton).
-template <int SOLVER>
+// TPB: the largest block size the calling kernel launches with (the grid search keeps
+// one column of shared-memory tables per thread).
+template <int SOLVER, int TPB>
 __device__ __forceinline__ void refraction_point(const DemView& d, const double A[3], const double B[3],
                                                  double na, double nb, int W, double out[3])
 {
     if constexpr (SOLVER == 0)
-        refraction_grid(d, A[0], A[1], A[2], B[0], B[1], B[2], na, nb, out);
+        refraction_grid<TPB>(d, A[0], A[1], A[2], B[0], B[1], B[2], na, nb, out);
     else
         refraction_newton(d, A, B, na, nb, W, out);
 }

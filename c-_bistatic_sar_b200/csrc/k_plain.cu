@@ -25,14 +25,14 @@ __global__ void k_dem_elevation(DemView d, const double2* __restrict__ xy, int64
 }
 
 template <int SOLVER>
-__global__ void k_refraction_points(DemView d, const double* __restrict__ p1, const double* __restrict__ p2,
+__global__ void __launch_bounds__(64) k_refraction_points(DemView d, const double* __restrict__ p1, const double* __restrict__ p2,
                                     int64_t n, double n1, double n2, int W, double* __restrict__ out)
 {
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
         double A[3] = {p1[3 * k], p1[3 * k + 1], p1[3 * k + 2]};
         double B[3] = {p2[3 * k], p2[3 * k + 1], p2[3 * k + 2]};
         double o[3];
-        refraction_point<SOLVER>(d, A, B, n1, n2, W, o);
+        refraction_point<SOLVER, 64>(d, A, B, n1, n2, W, o);
         out[3 * k] = o[0];
         out[3 * k + 1] = o[1];
         out[3 * k + 2] = o[2];
@@ -77,7 +77,7 @@ __device__ void reflection_point(const DemView& d, double txX, double txY, doubl
 
 // calculaSlantRangeFermat, src/raw_data_processing.cpp:112-255: one thread per pulse.
 template <int SOLVER>
-__global__ void k_slant_range(DemView d, const double* __restrict__ tx, const double* __restrict__ rx, int64_t np,
+__global__ void __launch_bounds__(64) k_slant_range(DemView d, const double* __restrict__ tx, const double* __restrict__ rx, int64_t np,
                               double Px, double Py, double Pz, double n1, double n2, int W,
                               double* __restrict__ ranges, double* __restrict__ ida, double* __restrict__ volta,
                               double* __restrict__ refl)
@@ -87,8 +87,8 @@ __global__ void k_slant_range(DemView d, const double* __restrict__ tx, const do
         double R[3] = {rx[3 * i], rx[3 * i + 1], rx[3 * i + 2]};
         double P[3] = {Px, Py, Pz};
         double a[3], b[3];
-        refraction_point<SOLVER>(d, T, P, n1, n2, W, a);   // :166-172
-        refraction_point<SOLVER>(d, P, R, n2, n1, W, b);   // :175-181
+        refraction_point<SOLVER, 64>(d, T, P, n1, n2, W, a);   // :166-172
+        refraction_point<SOLVER, 64>(d, P, R, n2, n1, W, b);   // :175-181
         for (int c = 0; c < 3; c++) {
             ida[3 * i + c] = a[c];
             volta[3 * i + c] = b[c];
@@ -136,8 +136,8 @@ __global__ void __launch_bounds__(128) k_bp_plain(BpArgs a)
                 const double T[3] = {__ldg(tx + 3 * i), __ldg(tx + 3 * i + 1), __ldg(tx + 3 * i + 2)};
                 const double R[3] = {__ldg(rx + 3 * i), __ldg(rx + 3 * i + 1), __ldg(rx + 3 * i + 2)};
                 double ia[3], vb[3];
-                refraction_point<SOLVER>(a.dem, T, P, a.n1, a.n2, a.W, ia);   // ida
-                refraction_point<SOLVER>(a.dem, P, R, a.n2, a.n1, a.W, vb);   // volta
+                refraction_point<SOLVER, 128>(a.dem, T, P, a.n1, a.n2, a.W, ia);   // ida
+                refraction_point<SOLVER, 128>(a.dem, P, R, a.n2, a.n1, a.W, vb);   // volta
                 double dx = P[0] - ia[0], dy = P[1] - ia[1], dz = P[2] - ia[2];
                 const double R2t = sqrt(dx * dx + dy * dy + dz * dz);          // :497-505
                 dx = P[0] - vb[0];
