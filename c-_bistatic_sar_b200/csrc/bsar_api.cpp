@@ -39,7 +39,9 @@ bsar_status bsar_create(bsar_ctx** out, const bsar_opts* opts)
     if (dev < 0 || dev >= count) return BSAR_ERR_INVALID_ARG;
     if (opts && opts->flags != 0) return BSAR_ERR_INVALID_ARG;
     if (cudaSetDevice(dev) != cudaSuccess) return BSAR_ERR_CUDA;
+    static std::atomic<uint64_t> serials{0};
     auto* ctx = new bsar_ctx();
+    ctx->serial = ++serials;
     ctx->device = dev;
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
         delete ctx;
@@ -84,16 +86,14 @@ void bsar_destroy(bsar_ctx* ctx)
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
-    clear_error(ctx);   // the destroying thread's entry; a later context may reuse the address
+    clear_error(ctx);   // the destroying thread's entry (others' carry the old serial)
     delete ctx;
 }
 
 const char* bsar_last_error(const bsar_ctx* ctx)
 {
     if (!ctx) return "null context";
-    auto& m = thread_errors();
-    auto it = m.find(ctx);
-    return it == m.end() ? "" : it->second.c_str();
+    return thread_error_message(ctx);
 }
 
 bsar_status bsar_set_stream(bsar_ctx* ctx, void* stream)

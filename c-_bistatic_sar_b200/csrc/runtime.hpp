@@ -14,6 +14,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -73,6 +74,7 @@ using namespace bsar_rt;
 struct DevBuf;
 
 struct bsar_ctx {
+    uint64_t serial = 0;   // unique per context in the process
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
@@ -159,13 +161,25 @@ inline void sync(bsar_ctx* ctx) { cuda_check(cudaStreamSynchronize(ctx->stream),
 // the message of the calling thread's latest call on that context, so threads sharing a
 // context (the reference calls its Fermat solver from up to 12 OpenMP threads) never read
 // a string another thread is rewriting.  A successful call clears the thread's entry.
-inline std::map<const bsar_ctx*, std::string>& thread_errors()
+// Entries carry the context's serial number, so a context created later at the address
+// of a destroyed one never shows an entry another thread left for the old one.
+struct ThreadError {
+    uint64_t serial;
+    std::string msg;
+};
+inline std::map<const bsar_ctx*, ThreadError>& thread_errors()
 {
-    thread_local std::map<const bsar_ctx*, std::string> m;
+    thread_local std::map<const bsar_ctx*, ThreadError> m;
     return m;
 }
-inline void set_error(const bsar_ctx* ctx, const std::string& msg) { thread_errors()[ctx] = msg; }
+inline void set_error(const bsar_ctx* ctx, const std::string& msg) { thread_errors()[ctx] = {ctx->serial, msg}; }
 inline void clear_error(const bsar_ctx* ctx) { thread_errors().erase(ctx); }
+inline const char* thread_error_message(const bsar_ctx* ctx)
+{
+    auto& m = thread_errors();
+    auto it = m.find(ctx);
+    return (it == m.end() || it->second.serial != ctx->serial) ? "" : it->second.msg.c_str();
+}
 
 // Runs an entry point's body with the context locked and its device current, turning
 // errors into a status and the calling thread's last error.

@@ -61,3 +61,34 @@ def test_last_error_is_per_thread(ctx):
     for t in ts:
         t.join()
     assert errors == []
+
+
+def test_last_error_not_inherited_by_a_later_context():
+    """A thread's failure on a context that another thread then destroys is not reported
+    for a context created afterwards, even one that reuses the freed address."""
+    a = bsar.Context(0)
+    seen, ctxs = {}, {"a": a}
+    failed, swapped = threading.Event(), threading.Event()
+
+    def worker():
+        try:
+            a.scene_release(10**12 + 7)
+        except bsar.BsarError:
+            pass
+        seen["a"] = a.last_error()
+        failed.set()
+        swapped.wait(60)
+        seen["b"] = ctxs["b"].last_error()          # same thread, the new context
+
+    t = threading.Thread(target=worker)
+    t.start()
+    failed.wait(60)
+    a.close()
+    ctxs["b"] = bsar.Context(0)
+    swapped.set()
+    t.join()
+    try:
+        assert "unknown scene id" in seen["a"]
+        assert seen["b"] == ""
+    finally:
+        ctxs["b"].close()
