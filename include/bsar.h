@@ -18,7 +18,8 @@
  *     in _device.
  *   - Every entry point returns a bsar_status; bsar_last_error(ctx) gives the message of
  *     the calling thread's latest call on ctx (empty after a success), so threads that
- *     share a context each read their own failure.
+ *     share a context each read their own failure.  The string stays valid until that
+ *     thread's next call on ctx.
  *     There is no CPU fallback: without a usable CUDA device bsar_create fails.
  *   - A context is internally locked; calls from several threads are serialised.
  */
