@@ -487,12 +487,23 @@ static void backproject(bsar_ctx* ctx, bsar_scene_id id, const bsar_grid* g, con
     if (o->legs != BSAR_LEGS_PER_PULSE) fail(BSAR_ERR_UNSUPPORTED, "the mixed forms use per-pulse legs");
     ensure_mixed_buffers(ctx);
     MixedReq r = mixed_request(s, a, o->precision == BSAR_MIXED_FP16);
+    // small grids: each tile's pulses in K chunks, so the work items fill the GPU
+    const int64_t vtiles = (a.v_count + 127) / 128;
+    const int K = mixed_chunks(a.v_count, a.np);
+    std::unique_ptr<DevBuf> partial, tile_done, chunks;
+    if (K > 1) {
+        partial = dev_alloc(ctx, sizeof(double2) * (size_t)K * (size_t)(g->nx * g->ny * g->nz));
+        tile_done = dev_alloc(ctx, sizeof(int) * (size_t)vtiles);
+        cuda_check(cudaMemsetAsync(tile_done->p, 0, sizeof(int) * (size_t)vtiles, ctx->stream), "memset");
+        const MixedChunks c{K, 0, partial->as<double2>(), tile_done->as<int>()};
+        chunks = dev_upload(ctx, &c, sizeof c);
+    }
     cuda_check(cudaMemcpyAsync(ctx->mixed_req->p, &r, sizeof r, cudaMemcpyHostToDevice, ctx->stream), "h2d");
     cuda_check(cudaMemsetAsync(ctx->mixed_counter->p, 0, sizeof(int), ctx->stream), "memset");
-    MixedBatch b{ctx->mixed_req->as<MixedReq>(), nullptr, nullptr, (int)((a.v_count + 127) / 128),
-                 ctx->mixed_counter->as<int>(), ctx->status->as<int>()};
+    MixedBatch b{ctx->mixed_req->as<MixedReq>(), nullptr, nullptr, (int)(vtiles * K),
+                 ctx->mixed_counter->as<int>(), ctx->status->as<int>(), chunks ? chunks->as<MixedChunks>() : nullptr};
     const int grid = (int)std::min<int64_t>(b.ntiles, mixed_grid_ctas());
-    cudaError_t e = launch_bp_mixed(b, a.W, grid, ctx->stream);
+    cudaError_t e = launch_bp_mixed(b, a.W, grid, ctx->stream, K > 1);
     launched(ctx, e, "back-projection (mixed)");
 }
 

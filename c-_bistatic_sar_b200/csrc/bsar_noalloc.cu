@@ -14,6 +14,9 @@
 //   per-pulse anchors (ref_L, ref_phase, ref_bin_i, ref_bin_f) and crossing offsets
 //   grid axes
 //   image (complex128, copied to the caller's buffer at the end)
+//   small grids only: the chunk record, pulse-chunk sums and per-tile chunk counts
+//   (cleared every call); the same chunking as the allocating entry point, so both
+//   give the same image
 //
 // The array is 64 MiB, and every GPU on which the library is loaded holds it until the
 // process exits.  It is one per device and per process and keeps the previous call's
@@ -77,7 +80,12 @@ extern "C" bsar_status bsar_backproject_mixed_noalloc(bsar_ctx* ctx, bsar_scene_
         const size_t o_off = o_anc + up256(20 * (size_t)np);
         const size_t o_axes = o_off + up256(32 * (size_t)np);
         const size_t o_img = o_axes + up256(8 * (size_t)(g->nx + g->ny + g->nz));
-        const size_t need = o_img + up256(16 * (size_t)nv);
+        const int64_t vtiles = (nv + 127) / 128;
+        const int K = mixed_chunks(nv, (int)np);
+        const size_t o_chk = o_img + up256(16 * (size_t)nv);
+        const size_t o_part = o_chk + (K > 1 ? up256(sizeof(MixedChunks)) : 0);
+        const size_t o_done = o_part + (K > 1 ? up256(16 * (size_t)K * (size_t)nv) : 0);
+        const size_t need = o_done + (K > 1 ? up256(4 * (size_t)vtiles) : 0);
         if (need > kScratchBytes)
             fail(BSAR_ERR_INVALID_ARG, "the call needs %zu bytes of scratch; the fixed scratch holds %zu", need,
                  kScratchBytes);
@@ -148,11 +156,18 @@ extern "C" bsar_status bsar_backproject_mixed_noalloc(bsar_ctx* ctx, bsar_scene_
         MixedReq r = mixed_request(s, a, o->precision == BSAR_MIXED_FP16);
         r.off_x = (float)(ox / (2.0 * np));
         r.off_y = (float)(oy / (2.0 * np));
+        MixedChunks* d_chunks = nullptr;
+        if (K > 1) {
+            const MixedChunks c{K, 0, reinterpret_cast<double2*>(S + o_part), reinterpret_cast<int*>(S + o_done)};
+            d_chunks = reinterpret_cast<MixedChunks*>(S + o_chk);
+            cuda_check(cudaMemcpyAsync(d_chunks, &c, sizeof c, cudaMemcpyHostToDevice, st), "chunk record");
+            cuda_check(cudaMemsetAsync(c.tile_done, 0, 4 * (size_t)vtiles, st), "clear chunk counts");
+        }
         MixedReq* d_req = reinterpret_cast<MixedReq*>(S + o_req);
         cuda_check(cudaMemcpyAsync(d_req, &r, sizeof r, cudaMemcpyHostToDevice, st), "request record");
-        MixedBatch b{d_req, nullptr, nullptr, (int)((nv + 127) / 128), counter, status};
+        MixedBatch b{d_req, nullptr, nullptr, (int)(vtiles * K), counter, status, d_chunks};
         const int grid = (int)std::min<int64_t>(b.ntiles, mixed_grid_ctas());
-        launched(ctx, launch_bp_mixed(b, a.W, grid, st), "back-projection (mixed, scratch)");
+        launched(ctx, launch_bp_mixed(b, a.W, grid, st, K > 1), "back-projection (mixed, scratch)");
         cuda_check(cudaMemcpyAsync(image_out, a.out, 16 * (size_t)nv, cudaMemcpyDeviceToHost, st), "image");
         int hstat = 0;
         cuda_check(cudaMemcpyAsync(&hstat, status, sizeof(int), cudaMemcpyDeviceToHost, st), "status");

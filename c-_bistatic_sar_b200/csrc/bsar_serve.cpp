@@ -28,6 +28,8 @@
 namespace {
 
 using Clock = std::chrono::steady_clock;
+// batch key bit: the batch holds a request whose tiles run in pulse chunks
+constexpr int kChunkedKey = 1 << 16;
 
 constexpr int kMaxSlots = 256;
 constexpr double kBatchTimeoutS = 300.0;   // bounded wait for one batch
@@ -53,11 +55,22 @@ struct Req {
     uint64_t reserved = 0;
     std::unique_ptr<Scene> scene;
     std::unique_ptr<DevBuf> axes, image;
+    std::unique_ptr<DevBuf> partial, tile_done;     // pulse-chunk sums of small grids
     MixedReq rec{};
+    MixedChunks chunks{};
     int64_t ntiles = 0, next_tile = 0, done_tiles = 0;
     Clock::time_point t_submit, t_done;
     double voxel_pulses = 0;
 };
+
+// Upper bound of the pulse-chunk buffers of a grid of nv voxels: at most 8 chunks per
+// 128-voxel tile, and chunks only while the tiles leave resident CTAs idle (fewer than
+// 4096 tiles on any device).  Host-only, so it does not ask the device.
+uint64_t chunk_bytes(uint64_t nv)
+{
+    const uint64_t tiles = (nv + 127) / 128;
+    return tiles < 4096 ? 16 * 8 * nv + 4 * tiles : 0;
+}
 
 uint64_t estimate_bytes(const Req& r)
 {
@@ -70,6 +83,7 @@ uint64_t estimate_bytes(const Req& r)
            + 16 * ns + 16 * nv                       // spectrum, image
            + 12 * nd + 48 * np + 52 * np             // DEM, trajectories, anchors
            + 24 * np * (uint64_t)std::max<int64_t>(r.n_scat, 1)   // synthesis work buffers
+           + chunk_bytes(nv)                         // pulse-chunk sums of a small grid
            + (1u << 20);
 }
 
@@ -77,12 +91,13 @@ uint64_t estimate_bytes(const Req& r)
 
 struct ServeBatch {
     MixedReq* h_reqs = nullptr;                     // pinned staging
+    MixedChunks* h_chunks = nullptr;
     int2* h_tiles = nullptr;
     int* h_ntiles = nullptr;
-    std::unique_ptr<DevBuf> d_reqs, d_tiles, d_ntiles, d_counter;
+    std::unique_ptr<DevBuf> d_reqs, d_chunks, d_tiles, d_ntiles, d_counter;
     cudaStream_t st = nullptr;
     cudaEvent_t ev = nullptr;
-    std::map<int, cudaGraphExec_t> graphs;          // per node-scan width W
+    std::map<int, cudaGraphExec_t> graphs;          // per node-scan width W (| kChunkedKey)
     std::vector<std::pair<Req*, int64_t>> items;    // requests in the batch, tiles each
     bool inflight = false;
     uint64_t seq = 0;
@@ -163,6 +178,8 @@ void release(bsar_server* s, Req* r)
         r->scene.reset();
         r->axes.reset();
         r->image.reset();
+        r->partial.reset();
+        r->tile_done.reset();
     });
 }
 
@@ -214,6 +231,14 @@ void admit(bsar_server* s, Req* r)
         a.v_begin = 0;
         a.v_count = nv;
         a.out = r->image->as<double2>();
+        // small grids: each tile's pulses in K chunks (the rule every path applies)
+        const int64_t vtiles = (nv + 127) / 128;
+        const int K = mixed_chunks(nv, (int)sc->np);
+        if (K > 1) {
+            r->partial = dev_alloc(ctx, sizeof(double2) * (size_t)K * (size_t)nv);
+            r->tile_done = dev_alloc(ctx, sizeof(int) * (size_t)vtiles);
+            cuda_check(cudaMemsetAsync(r->tile_done->p, 0, sizeof(int) * (size_t)vtiles, ctx->stream), "memset");
+        }
         bsar_grid g = r->grid;
         g.x_axis = r->gx.data();
         g.y_axis = r->gy.data();
@@ -221,7 +246,8 @@ void admit(bsar_server* s, Req* r)
         set_anchors(ctx, sc, &g, a);
         sync(ctx);
         r->rec = mixed_request(sc, a, r->opts.precision == BSAR_MIXED_FP16);
-        r->ntiles = (nv + 127) / 128;
+        if (K > 1) r->chunks = MixedChunks{K, 0, r->partial->as<double2>(), r->tile_done->as<int>()};
+        r->ntiles = vtiles * K;             // work items: (tile, chunk) pairs
         r->voxel_pulses = (double)nv * (double)sc->np;
     });
 }
@@ -249,7 +275,9 @@ int build_batch(bsar_server* s, ServeBatch& b, int* W_out)
         progress = false;
         for (Req* r : live) {
             int64_t take = std::min<int64_t>({(int64_t)chunk, r->ntiles - r->next_tile, (int64_t)(s->max_tiles - n)});
-            for (int64_t t = 0; t < take; t++) list.push_back({r->rec.a.np, r->slot, (int)(r->next_tile + t)});
+            // a work item's cost follows the pulses of its chunk
+            const int cost = r->rec.a.np / std::max(1, r->chunks.nchunk);
+            for (int64_t t = 0; t < take; t++) list.push_back({cost, r->slot, (int)(r->next_tile + t)});
             if (take > 0) {
                 n += (int)take;
                 r->next_tile += take;
@@ -263,11 +291,16 @@ int build_batch(bsar_server* s, ServeBatch& b, int* W_out)
     }
     std::stable_sort(list.begin(), list.end(), [](const Item& x, const Item& y) { return x.np > y.np; });
     for (int k = 0; k < n; k++) b.h_tiles[k] = make_int2(list[k].slot, list[k].tile);
-    for (Req* r : s->active) b.h_reqs[r->slot] = r->rec;
+    for (Req* r : s->active) {
+        b.h_reqs[r->slot] = r->rec;
+        b.h_chunks[r->slot] = r->chunks;
+    }
     *b.h_ntiles = n;
     for (Req* r : s->active)
         if (per_req.count(r)) b.items.push_back({r, per_req[r]});
-    *W_out = mixedW ? 0 : W;
+    bool chunked = false;
+    for (const auto& it : b.items) chunked = chunked || it.first->chunks.nchunk > 1;
+    *W_out = (mixedW ? 0 : W) | (chunked ? kChunkedKey : 0);
     return n;
 }
 
@@ -277,14 +310,15 @@ cudaGraphExec_t batch_graph(bsar_server* s, ServeBatch& bt, int W)
     auto it = bt.graphs.find(W);
     if (it != bt.graphs.end()) return it->second;
     MixedBatch b{bt.d_reqs->as<MixedReq>(), bt.d_tiles->as<int2>(), bt.d_ntiles->as<int>(), 0,
-                 bt.d_counter->as<int>(), s->ctx->status->as<int>()};
+                 bt.d_counter->as<int>(), s->ctx->status->as<int>(), bt.d_chunks->as<MixedChunks>()};
     cudaGraph_t g = nullptr;
     cuda_check(cudaStreamBeginCapture(bt.st, cudaStreamCaptureModeThreadLocal), "begin capture");
     cudaMemcpyAsync(bt.d_reqs->p, bt.h_reqs, sizeof(MixedReq) * kMaxSlots, cudaMemcpyHostToDevice, bt.st);
+    cudaMemcpyAsync(bt.d_chunks->p, bt.h_chunks, sizeof(MixedChunks) * kMaxSlots, cudaMemcpyHostToDevice, bt.st);
     cudaMemcpyAsync(bt.d_tiles->p, bt.h_tiles, sizeof(int2) * s->max_tiles, cudaMemcpyHostToDevice, bt.st);
     cudaMemcpyAsync(bt.d_ntiles->p, bt.h_ntiles, sizeof(int), cudaMemcpyHostToDevice, bt.st);
     cudaMemsetAsync(bt.d_counter->p, 0, sizeof(int), bt.st);
-    cudaError_t le = launch_bp_mixed(b, W, s->grid_ctas, bt.st);
+    cudaError_t le = launch_bp_mixed(b, W & ~kChunkedKey, s->grid_ctas, bt.st, (W & kChunkedKey) != 0);
     cudaError_t ce = cudaStreamEndCapture(bt.st, &g);
     cuda_check(le, "batch launch (capture)");
     cuda_check(ce, "end capture");
@@ -301,12 +335,16 @@ void launch_batch(bsar_server* s, ServeBatch& bt, int W, int n)
         cuda_check(cudaGraphLaunch(batch_graph(s, bt, W), bt.st), "graph launch");
     } else {
         MixedBatch b{bt.d_reqs->as<MixedReq>(), bt.d_tiles->as<int2>(), nullptr, n, bt.d_counter->as<int>(),
-                     s->ctx->status->as<int>()};
+                     s->ctx->status->as<int>(), bt.d_chunks->as<MixedChunks>()};
         cuda_check(cudaMemcpyAsync(bt.d_reqs->p, bt.h_reqs, sizeof(MixedReq) * kMaxSlots, cudaMemcpyHostToDevice, bt.st),
+                   "h2d");
+        cuda_check(cudaMemcpyAsync(bt.d_chunks->p, bt.h_chunks, sizeof(MixedChunks) * kMaxSlots, cudaMemcpyHostToDevice,
+                                   bt.st),
                    "h2d");
         cuda_check(cudaMemcpyAsync(bt.d_tiles->p, bt.h_tiles, sizeof(int2) * n, cudaMemcpyHostToDevice, bt.st), "h2d");
         cuda_check(cudaMemsetAsync(bt.d_counter->p, 0, sizeof(int), bt.st), "memset");
-        cuda_check(launch_bp_mixed(b, W, std::min(n, s->grid_ctas), bt.st), "batch launch");
+        cuda_check(launch_bp_mixed(b, W & ~kChunkedKey, std::min(n, s->grid_ctas), bt.st, (W & kChunkedKey) != 0),
+                   "batch launch");
     }
     cuda_check(cudaEventRecord(bt.ev, bt.st), "event");
     bt.inflight = true;
@@ -543,10 +581,13 @@ bsar_status bsar_server_create(bsar_ctx* ctx, const bsar_server_opts* opts, bsar
             cuda_check(cudaStreamCreateWithPriority(&bt.st, cudaStreamNonBlocking, least), "stream");
             cuda_check(cudaEventCreateWithFlags(&bt.ev, cudaEventDisableTiming), "event");
             cuda_check(cudaMallocHost((void**)&bt.h_reqs, sizeof(MixedReq) * kMaxSlots), "pinned");
+            cuda_check(cudaMallocHost((void**)&bt.h_chunks, sizeof(MixedChunks) * kMaxSlots), "pinned");
+            std::memset(bt.h_chunks, 0, sizeof(MixedChunks) * kMaxSlots);
             cuda_check(cudaMallocHost((void**)&bt.h_tiles, sizeof(int2) * s->max_tiles), "pinned");
             cuda_check(cudaMallocHost((void**)&bt.h_ntiles, sizeof(int)), "pinned");
             std::memset(bt.h_reqs, 0, sizeof(MixedReq) * kMaxSlots);
             bt.d_reqs = dev_alloc(ctx, sizeof(MixedReq) * kMaxSlots);
+            bt.d_chunks = dev_alloc(ctx, sizeof(MixedChunks) * kMaxSlots);
             bt.d_tiles = dev_alloc(ctx, sizeof(int2) * s->max_tiles);
             bt.d_ntiles = dev_alloc(ctx, sizeof(int));
             bt.d_counter = dev_alloc(ctx, sizeof(int));
@@ -709,16 +750,20 @@ void bsar_server_destroy(bsar_server* s)
             kv.second->scene.reset();
             kv.second->axes.reset();
             kv.second->image.reset();
+            kv.second->partial.reset();
+            kv.second->tile_done.reset();
         }
         if (s->io) cudaStreamSynchronize(s->io);
         s->ctx->stream = saved;
         for (ServeBatch& bt : s->batch) {
             for (auto& kv : bt.graphs) cudaGraphExecDestroy(kv.second);
             bt.d_reqs.reset();
+            bt.d_chunks.reset();
             bt.d_tiles.reset();
             bt.d_ntiles.reset();
             bt.d_counter.reset();
             if (bt.h_reqs) cudaFreeHost(bt.h_reqs);
+            if (bt.h_chunks) cudaFreeHost(bt.h_chunks);
             if (bt.h_tiles) cudaFreeHost(bt.h_tiles);
             if (bt.h_ntiles) cudaFreeHost(bt.h_ntiles);
             if (bt.ev) cudaEventDestroy(bt.ev);

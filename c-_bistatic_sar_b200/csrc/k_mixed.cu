@@ -704,13 +704,14 @@ __device__ __forceinline__ MixedCtx req_ctx(const MixedReq& r)
     return m;
 }
 
-// One voxel of a request over all its pulses (k: index in the request's voxel range;
+// One voxel of a request over pulses [p0, p1) (k: index in the request's voxel range;
 // k >= v_count repeats the last voxel without storing it, so whole warps stay active).
-template <int WT>
+// The sum goes to dst at the voxel's image index.
+template <int WT, bool CH>
 __device__ __forceinline__ void voxel_mixed(const BpArgs& a, const MixedCtx& m, const Tile& T, float2* table_buf,
-                                            bool fp16, int64_t kk)
+                                            bool fp16, int64_t kk, int p0, int p1, double2* __restrict__ dst)
 {
-    const int np = a.np;
+    const int np = CH ? p1 : a.np;
     const float k_bin = (float)(a.fs_eff / a.c);
     const float k_phase = (float)(2.0 * 3.14159265358979323846 / a.lambda);
     const float n1f = (float)a.n1, n2f = (float)a.n2;
@@ -724,7 +725,7 @@ __device__ __forceinline__ void voxel_mixed(const BpArgs& a, const MixedCtx& m, 
     const float P32[3] = {(float)(P[0] - m.ox), (float)(P[1] - m.oy), (float)P[2]};
     const VoxelStart vs{height32(m, P32[0], P32[1]), dem_elevation(a.dem, P[0], P[1])};
     float accr = 0.f, acci = 0.f, cmpr = 0.f, cmpi = 0.f;
-    for (int i = 0; i < np; i++) {
+    for (int i = CH ? p0 : 0; i < np; i++) {
         const double Tx[3] = {__ldg(a.tx + 3 * i), __ldg(a.tx + 3 * i + 1), __ldg(a.tx + 3 * i + 2)};
         const double Rx[3] = {__ldg(a.rx + 3 * i), __ldg(a.rx + 3 * i + 1), __ldg(a.rx + 3 * i + 2)};
         const float T32[3] = {(float)(Tx[0] - m.ox), (float)(Tx[1] - m.oy), (float)Tx[2]};
@@ -797,8 +798,29 @@ __device__ __forceinline__ void voxel_mixed(const BpArgs& a, const MixedCtx& m, 
         }
     }
     if (kk < a.v_count)
-        a.out[((int64_t)xi * a.ny + yi) * a.nz + zi] =
+        (CH ? dst : a.out)[((int64_t)xi * a.ny + yi) * a.nz + zi] =
             make_double2((double)accr - (double)cmpr, (double)acci - (double)cmpi);
+}
+
+// The last of a tile's pulse chunks to finish adds the chunks' sums, in chunk order, into
+// the image (partial sums of the other CTAs are read from L2).
+__device__ __forceinline__ void reduce_chunks(const BpArgs& a, const double2* __restrict__ partial, int K,
+                                              int64_t kk)
+{
+    if (kk >= a.v_count) return;
+    const int64_t v = a.v_begin + kk;
+    const int yi = (int)(v % a.ny);
+    const int xi = (int)((v / a.ny) % a.nx);
+    const int zi = (int)(v / ((int64_t)a.nx * a.ny));
+    const int64_t idx = ((int64_t)xi * a.ny + yi) * a.nz + zi;
+    const int64_t nvox = (int64_t)a.nx * a.ny * a.nz;
+    double sr = 0.0, si = 0.0;
+    for (int c = 0; c < K; c++) {
+        const double2 q = __ldcg(partial + c * nvox + idx);
+        sr += q.x;
+        si += q.y;
+    }
+    a.out[idx] = make_double2(sr, si);
 }
 
 }  // namespace
@@ -808,13 +830,14 @@ __device__ __forceinline__ void voxel_mixed(const BpArgs& a, const MixedCtx& m, 
 // list is exhausted, so tiles of several requests share one launch.  The 128 voxels of a
 // work item are the same 128 a one-request launch gives a CTA, so a voxel's arithmetic
 // (warp tables, DEM tile, sums) does not depend on what else is in the batch.
-template <int WT>
+template <int WT, bool CH>
 __global__ void __launch_bounds__(128, 4) k_bp_mixed(MixedBatch b)
 {
     __shared__ alignas(128) float tile_s[TI * TJ];
     __shared__ alignas(16) float2 air_s[4][TableRows<WT>::v * TBJ];   // one (z, E-leg) table per warp
     __shared__ alignas(8) uint64_t mbar;
     __shared__ int2 work;
+    __shared__ int last_chunk;
     float2* table_buf = air_s[threadIdx.x >> 5];
     const int ntiles = b.ntiles_dev ? *b.ntiles_dev : b.ntiles;
     if (threadIdx.x == 0) {
@@ -836,10 +859,14 @@ __global__ void __launch_bounds__(128, 4) k_bp_mixed(MixedBatch b)
         const MixedReq& R = b.reqs[w.x];
         const BpArgs& a = R.a;
         const MixedCtx m = req_ctx(R);
+        // work item -> (128-voxel tile, pulse chunk); the unchunked kernel has one chunk
+        const int K = CH ? max(b.chunks[w.x].nchunk, 1) : 1;
+        const int tile = CH ? w.y / K : w.y;
+        const int chunk = CH ? w.y - tile * K : 0;
         Tile T{tile_s, 0, 0, false};
         if (R.use_tile && !copy_pending) {
             // DEM tile centred on this work item's voxels plus the mean crossing offset
-            const int64_t v0 = a.v_begin + (int64_t)w.y * 128;
+            const int64_t v0 = a.v_begin + (int64_t)tile * 128;
             const int64_t vl = min(v0 + 128, a.v_begin + a.v_count) - 1;
             const int64_t vm = (v0 + vl) / 2;
             const double cx = __ldg(a.gx + (int)((vm / a.ny) % a.nx)) + R.off_x;
@@ -851,7 +878,28 @@ __global__ void __launch_bounds__(128, 4) k_bp_mixed(MixedBatch b)
             parity ^= 1u;
             copy_pending = !T.ok;
         }
-        voxel_mixed<WT>(a, m, T, table_buf, R.fp16 != 0, (int64_t)w.y * 128 + threadIdx.x);
+        if constexpr (!CH) {
+            voxel_mixed<WT, false>(a, m, T, table_buf, R.fp16 != 0, (int64_t)w.y * 128 + threadIdx.x, 0, 0, nullptr);
+        } else {
+            const int p0 = (int)((int64_t)chunk * a.np / K), p1 = (int)((int64_t)(chunk + 1) * a.np / K);
+            double2* dst = K == 1 ? a.out : b.chunks[w.x].partial + chunk * ((int64_t)a.nx * a.ny * a.nz);
+            voxel_mixed<WT, true>(a, m, T, table_buf, R.fp16 != 0, (int64_t)tile * 128 + threadIdx.x, p0, p1, dst);
+            // the work item again from shared memory, so none of it stays live over the pulses
+            const volatile int* wv = reinterpret_cast<volatile int*>(&work);
+            const int2 w2 = make_int2(wv[0], wv[1]);
+            const MixedChunks C = b.chunks[w2.x];
+            if (C.nchunk > 1) {
+                const int tile2 = w2.y / C.nchunk;
+                __threadfence();   // this chunk's sums before the count that publishes them
+                __syncthreads();
+                if (threadIdx.x == 0) last_chunk = atomicAdd(C.tile_done + tile2, 1) == C.nchunk - 1;
+                __syncthreads();
+                if (last_chunk) {
+                    __threadfence();
+                    reduce_chunks(b.reqs[w2.x].a, C.partial, C.nchunk, (int64_t)tile2 * 128 + threadIdx.x);
+                }
+            }
+        }
     }
     if (copy_pending) drain_tile(&mbar, parity ^ 1u);
 }
@@ -906,14 +954,14 @@ cudaError_t launch_refraction_mixed(const DemView& d, int pitch, const double* p
 
 // Shared-memory carve-out for 4 resident CTAs per SM (DEM tile + 4 warp tables each),
 // set once per device; the rest of the unified L1 stays cache for the sample gathers.
-template <int WT> static void set_carveout()
+template <int WT, bool CH> static void set_carveout()
 {
     cudaFuncAttributes fa{};
-    if (cudaFuncGetAttributes(&fa, k_bp_mixed<WT>) != cudaSuccess) return;
+    if (cudaFuncGetAttributes(&fa, k_bp_mixed<WT, CH>) != cudaSuccess) return;
     const double need = 4.0 * (double)(fa.sharedSizeBytes + 1024);
     int pct = (int)(100.0 * need / (228.0 * 1024.0)) + 1;
     pct = pct > 100 ? 100 : pct;
-    cudaFuncSetAttribute(k_bp_mixed<WT>, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+    cudaFuncSetAttribute(k_bp_mixed<WT, CH>, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
 }
 
 static void mixed_setup_device()
@@ -923,11 +971,26 @@ static void mixed_setup_device()
     cudaGetDevice(&dev);
     const uint64_t bit = 1ull << (dev & 63);
     if (done.load() & bit) return;
-    set_carveout<0>();
-    set_carveout<3>();
-    set_carveout<6>();
-    set_carveout<12>();
+    set_carveout<0, false>();
+    set_carveout<3, false>();
+    set_carveout<6, false>();
+    set_carveout<12, false>();
+    set_carveout<0, true>();
+    set_carveout<3, true>();
+    set_carveout<6, true>();
+    set_carveout<12, true>();
     done.fetch_or(bit);
+}
+
+int mixed_chunks(int64_t voxels, int pulses)
+{
+    const int64_t tiles = (voxels + 127) / 128;
+    const int64_t ctas = mixed_grid_ctas();
+    if (tiles <= 0 || pulses < 2 || tiles * 2 > ctas) return 1;
+    int64_t k = ctas / tiles;
+    if (k > 8) k = 8;
+    if (k > pulses) k = pulses;
+    return (int)k;
 }
 
 int mixed_grid_ctas()
@@ -938,21 +1001,29 @@ int mixed_grid_ctas()
         int dev = 0, sms = 148, per = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_bp_mixed<6>, 128, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_bp_mixed<6, false>, 128, 0);
         ctas = sms * (per > 0 ? per : 1);
     }
     return ctas;
 }
 
-cudaError_t launch_bp_mixed(const MixedBatch& b, int W, int grid, cudaStream_t st)
+template <bool CH> static void launch_w(const MixedBatch& b, int W, int grid, cudaStream_t st)
+{
+    switch (W) {
+    case 3: k_bp_mixed<3, CH><<<grid, 128, 0, st>>>(b); break;
+    case 6: k_bp_mixed<6, CH><<<grid, 128, 0, st>>>(b); break;
+    case 12: k_bp_mixed<12, CH><<<grid, 128, 0, st>>>(b); break;
+    default: k_bp_mixed<0, CH><<<grid, 128, 0, st>>>(b); break;
+    }
+}
+
+cudaError_t launch_bp_mixed(const MixedBatch& b, int W, int grid, cudaStream_t st, bool chunked)
 {
     mixed_setup_device();
-    switch (W) {
-    case 3: k_bp_mixed<3><<<grid, 128, 0, st>>>(b); break;
-    case 6: k_bp_mixed<6><<<grid, 128, 0, st>>>(b); break;
-    case 12: k_bp_mixed<12><<<grid, 128, 0, st>>>(b); break;
-    default: k_bp_mixed<0><<<grid, 128, 0, st>>>(b); break;
-    }
+    if (chunked)
+        launch_w<true>(b, W, grid, st);
+    else
+        launch_w<false>(b, W, grid, st);
     return cudaGetLastError();
 }
 

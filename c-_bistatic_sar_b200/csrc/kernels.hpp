@@ -104,6 +104,18 @@ struct alignas(64) MixedReq {
     float pad2;
 };
 
+// Pulse chunks of a request (kept beside MixedReq, read only by the chunked kernel).
+// nchunk > 1: work item t of the request is chunk t % nchunk of tile t / nchunk; each
+// chunk writes its voxels' sums to partial[chunk * (nx ny nz) + image index], and the last
+// of a tile's chunks to finish (counted in tile_done[tile], zero before the request's first
+// launch) adds the chunks, in chunk order, into the image.
+struct MixedChunks {
+    int nchunk;           // <= 1: the whole pulse range in one work item
+    int pad;
+    double2* partial;
+    int* tile_done;
+};
+
 // A batch of the persistent mixed kernel: `ntiles` work items (request index, tile of 128
 // voxels in the request's flat voxel order); tiles == null means request 0, tiles 0..n-1.
 struct MixedBatch {
@@ -113,18 +125,25 @@ struct MixedBatch {
     int ntiles;
     int* counter;            // zeroed before the launch
     int* status;             // device status word (1 = a tile copy timed out)
+    const MixedChunks* chunks;   // per request, indexed as reqs (the chunked kernel only)
 };
 
 cudaError_t launch_bp_plain(const BpArgs& a, int solver, int legs, cudaStream_t st);
 cudaError_t launch_refraction_mixed(const DemView& d, int pitch, const double* p1, const double* p2, int64_t n,
                                     double n1, double n2, int W, double* out, cudaStream_t st);
-cudaError_t launch_bp_mixed(const MixedBatch& b, int W, int grid, cudaStream_t st);
+// chunked: some request of the batch has nchunk > 1 (the kernel with the chunk sums)
+cudaError_t launch_bp_mixed(const MixedBatch& b, int W, int grid, cudaStream_t st, bool chunked);
 float mixed_start_band(const DemView& d);
 // batched tiled transpose: out[b][c][r] = in[b][r][c] (complex128), and real -> complex128
 cudaError_t launch_transpose_c128(const double2* in, double2* out, int64_t R, int64_t C, int64_t in_ld, int64_t out_ld,
                                   int64_t in_bs, int64_t out_bs, int64_t batch, cudaStream_t st);
 cudaError_t launch_real_to_c128(const double* in, double2* out, int64_t n, cudaStream_t st);
 int mixed_grid_ctas();   // persistent grid size (SMs x resident CTAs)
+// Pulse chunks per 128-voxel tile for a request of `voxels` voxels and `pulses` pulses:
+// as many as keep the request's work items within one wave of resident CTAs (at most 8
+// and at most the pulse count); 1 for grids that already fill the GPU.  A property of the
+// request and the device only, so every path gives the same request the same image.
+int mixed_chunks(int64_t voxels, int pulses);
 cudaError_t launch_ref_ranges(const DemView& d, const double* tx, const double* rx, int np, const double* center,
                               double n1, double n2, int W, double lambda, double bin_per_m, double* ref_L,
                               float* ref_phase, int* ref_bin_i, float* ref_bin_f, double* offsets, cudaStream_t st);

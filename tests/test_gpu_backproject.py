@@ -92,6 +92,31 @@ def test_mixed_matches_fp64(ctx, which, precision, request):
     assert np.argmax(np.abs(img)) == np.argmax(np.abs(ref))
 
 
+@pytest.mark.parametrize("which", ["small", "rough"])
+def test_mixed_small_grid_pulse_chunks_are_deterministic(ctx, which, request):
+    """Grids too small to fill the GPU run each 128-voxel tile's pulses in chunks; the
+    last chunk of a tile to finish adds the chunks in chunk order.  Whatever order the
+    chunks finish in, repeated runs give the same bits, through the device-buffer entry
+    point as well as the host one."""
+    import torch
+
+    sc = request.getfixturevalue(which)
+    sid = bsar.upload_scene(ctx, sc)
+    try:
+        imgs = [ctx.backproject(sid, sc.gx, sc.gy, sc.gz, solver="newton", legs="per_pulse", precision="mixed")
+                for _ in range(4)]
+        nv = len(sc.gx) * len(sc.gy) * len(sc.gz)
+        d = torch.empty((nv, 2), dtype=torch.float64, device="cuda")
+        ctx.backproject_device(sid, sc.gx, sc.gy, sc.gz, d.data_ptr(), solver="newton", legs="per_pulse",
+                               precision="mixed")
+        ctx.synchronize()
+        dev = d.cpu().numpy().view(np.complex128).reshape(imgs[0].shape)
+    finally:
+        ctx.scene_release(sid)
+    for img in imgs[1:] + [dev]:
+        assert np.array_equal(img, imgs[0])
+
+
 def test_scatterer_focuses_at_its_voxel(ctx):
     spec = S.scaled(S.config_spec(1), n_pulses=64, nx=15, ny=15, nz=9, dxy=0.04, dz=0.08, n_scatterers=1,
                     snr_db=np.inf)

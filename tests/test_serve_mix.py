@@ -39,8 +39,8 @@ def test_poisson_arrivals():
 
 def test_server_estimate_counts_request_buffers():
     """bsar_server_estimate (host only): the bytes a request reserves grow with its
-    pulses x samples (raw + upsampled pulses), its voxels (image) and its scatterers, and
-    FP16 storage halves the upsampled part."""
+    pulses x samples (raw + upsampled pulses), its voxels (image and, for small grids, the
+    pulse-chunk sums) and its scatterers, and FP16 storage halves the upsampled part."""
     import bsar
 
     m = S.serve_mix(1, side=(21, 21), pulses=(128, 128), samples_log2=(11, 11), scatterers=(5, 5))
@@ -58,6 +58,9 @@ def test_server_estimate_counts_request_buffers():
     up = 4
     assert est(np_=256) - base == 128 * (16 * 2048 + 8 * 2048 * up + 48 + 52 + 24 * 5)
     assert est(ns=4096) - base == 128 * (16 * 2048 + 8 * 2048 * up) + 16 * 2048
-    assert est(nx=42) - base == 16 * (42 ** 3 - 21 ** 3)
+    # image, plus the pulse-chunk bound of small grids (8 chunk sums per voxel, one count
+    # per 128-voxel tile)
+    tiles = lambda n: -(-n ** 3 // 128)
+    assert est(nx=42) - base == (16 + 128) * (42 ** 3 - 21 ** 3) + 4 * (tiles(42) - tiles(21))
     assert est(nscat=10) - base == 24 * 128 * 5
     assert base - est(precision="mixed_fp16") == 4 * 128 * 2048 * up
