@@ -984,12 +984,13 @@ static void mixed_setup_device()
 
 int mixed_chunks(int64_t voxels, int pulses)
 {
+    constexpr int kMinChunkPulses = 128;   // below this a chunk's fixed cost (DEM tile, start heights) shows
     const int64_t tiles = (voxels + 127) / 128;
     const int64_t ctas = mixed_grid_ctas();
-    if (tiles <= 0 || pulses < 2 || tiles * 2 > ctas) return 1;
+    if (tiles <= 0 || pulses < 2 * kMinChunkPulses || tiles * 2 > ctas) return 1;
     int64_t k = ctas / tiles;
     if (k > 8) k = 8;
-    if (k > pulses) k = pulses;
+    if (k > pulses / kMinChunkPulses) k = pulses / kMinChunkPulses;
     return (int)k;
 }
 

@@ -140,8 +140,8 @@ cudaError_t launch_transpose_c128(const double2* in, double2* out, int64_t R, in
 cudaError_t launch_real_to_c128(const double* in, double2* out, int64_t n, cudaStream_t st);
 int mixed_grid_ctas();   // persistent grid size (SMs x resident CTAs)
 // Pulse chunks per 128-voxel tile for a request of `voxels` voxels and `pulses` pulses:
-// as many as keep the request's work items within one wave of resident CTAs (at most 8
-// and at most the pulse count); 1 for grids that already fill the GPU.  A property of the
+// as many as keep the request's work items within one wave of resident CTAs, at most 8
+// and with at least 128 pulses each; 1 for grids that already fill the GPU.  A property of the
 // request and the device only, so every path gives the same request the same image.
 int mixed_chunks(int64_t voxels, int pulses);
 cudaError_t launch_ref_ranges(const DemView& d, const double* tx, const double* rx, int np, const double* center,

@@ -31,6 +31,12 @@ def small():
 
 
 @pytest.fixture(scope="module")
+def chunked():
+    # 405 voxels (4 tiles) and 256 pulses: the mixed kernel runs each tile in 2 pulse chunks
+    return _setup(S.scaled(S.config_spec(1), n_pulses=256, nx=9, ny=9, nz=5, dxy=0.16, dz=0.32))
+
+
+@pytest.fixture(scope="module")
 def rough():
     return _setup(S.scaled(S.config_spec(2), n_pulses=48, n_samples=4096, nx=11, ny=11, nz=6, dxy=0.1, dz=0.1,
                            n_scatterers=4))
@@ -78,7 +84,7 @@ def test_plain_newton_matches_oracle(ctx, oracle, which, request):
 
 
 @pytest.mark.parametrize("precision", ["mixed", "mixed_fp16"])
-@pytest.mark.parametrize("which", ["small", "rough", "large"])
+@pytest.mark.parametrize("which", ["small", "chunked", "rough", "large"])
 def test_mixed_matches_fp64(ctx, which, precision, request):
     sc = request.getfixturevalue(which)
     sid = bsar.upload_scene(ctx, sc)
@@ -92,7 +98,7 @@ def test_mixed_matches_fp64(ctx, which, precision, request):
     assert np.argmax(np.abs(img)) == np.argmax(np.abs(ref))
 
 
-@pytest.mark.parametrize("which", ["small", "rough"])
+@pytest.mark.parametrize("which", ["chunked"])
 def test_mixed_small_grid_pulse_chunks_are_deterministic(ctx, which, request):
     """Grids too small to fill the GPU run each 128-voxel tile's pulses in chunks; the
     last chunk of a tile to finish adds the chunks in chunk order.  Whatever order the

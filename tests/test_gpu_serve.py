@@ -21,7 +21,8 @@ pytestmark = pytest.mark.gpu
 
 
 def _mix(n, seed=11, **kw):
-    args = dict(side=(9, 25), pulses=(32, 96), samples_log2=(11, 12), scatterers=(3, 8))
+    # up to 320 pulses: the small grids with 256 or more run in pulse chunks
+    args = dict(side=(9, 25), pulses=(32, 320), samples_log2=(11, 12), scatterers=(3, 8))
     args.update(kw)
     return S.serve_mix(n, seed=S.SEED_BASE + seed, n_dems=3, **args)
 

@@ -17,12 +17,21 @@ def scene():
                                  dz=0.1, n_scatterers=4))
 
 
+@pytest.fixture(scope="module")
+def chunked_scene():
+    # small grid, 256 pulses: both entry points run it in pulse chunks
+    return S.make_scene(S.scaled(S.config_spec(2), n_pulses=256, n_samples=4096, nx=13, ny=11, nz=6, dxy=0.1,
+                                 dz=0.1, n_scatterers=4))
+
+
 def _alloc(ctx, sid, gx, gy, gz, precision):
     return ctx.backproject(sid, gx, gy, gz, solver="newton", legs="per_pulse", precision=precision)
 
 
+@pytest.mark.parametrize("which", ["scene", "chunked_scene"])
 @pytest.mark.parametrize("precision", ["mixed", "mixed_fp16"])
-def test_noalloc_matches_allocating_entry_point(ctx, scene, precision):
+def test_noalloc_matches_allocating_entry_point(ctx, which, precision, request):
+    scene = request.getfixturevalue(which)
     sid = bsar.upload_scene(ctx, scene)
     try:
         ctx.scene_compress(sid, precision)
