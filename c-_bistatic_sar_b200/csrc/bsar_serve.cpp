@@ -4,8 +4,9 @@
 // stream, pinned staging and device copies, keep up to two batches in flight:
 //
 //   loop:
-//     fill every idle batch slot: a fair-share list of (request, 128-voxel tile) work
-//       items of the admitted requests, longest tiles first, launched as a replay of a
+//     fill every idle batch slot: a fair-share list of (request, work item) pairs --
+//       a 128-voxel tile, or one pulse chunk of a tile for small grids -- of the admitted
+//       requests, most costly items first, launched as a replay of a
 //       captured CUDA graph (request records and tile list copied from pinned staging,
 //       work counter zeroed, persistent mixed kernel)
 //     wait for the older batch (bounded); while it runs, admit pending requests FIFO
@@ -16,8 +17,8 @@
 //       resources released, latency recorded)
 //
 // The second batch's CTAs take the SMs the first batch's tail leaves idle.  Work items
-// are the same 128-voxel groups a one-request launch uses, so every voxel's arithmetic
-// is independent of the batch it runs in.
+// are the same 128-voxel groups (and pulse chunks) a one-request launch uses, so every
+// voxel's arithmetic is independent of the batch it runs in.
 #include "runtime.hpp"
 
 #include <chrono>

@@ -830,6 +830,9 @@ __device__ __forceinline__ void reduce_chunks(const BpArgs& a, const double2* __
 // list is exhausted, so tiles of several requests share one launch.  The 128 voxels of a
 // work item are the same 128 a one-request launch gives a CTA, so a voxel's arithmetic
 // (warp tables, DEM tile, sums) does not depend on what else is in the batch.
+// CH: the instantiation for batches holding small-grid requests whose tiles run in pulse
+// chunks (MixedChunks); the last chunk of a tile to finish adds the chunks' sums in chunk
+// order.  Batches without chunks run the other instantiation, which never reads them.
 template <int WT, bool CH>
 __global__ void __launch_bounds__(128, 4) k_bp_mixed(MixedBatch b)
 {
