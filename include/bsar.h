@@ -364,8 +364,10 @@ typedef struct bsar_server_stats {
  * request completes. */
 bsar_status bsar_server_create(bsar_ctx* ctx, const bsar_server_opts* opts, bsar_server** out);
 bsar_status bsar_server_submit(bsar_server* srv, const bsar_request* req, bsar_request_id* out);
-/* Device bytes a request reserves against the server's budget while admitted.  A
- * request above the whole budget fails with BSAR_ERR_OOM_BUDGET; smaller ones wait. */
+/* Device bytes a request reserves against the server's budget while admitted (an upper
+ * bound: it includes the pulse-chunk sums a small grid may use, computed without asking
+ * the device).  A request above the whole budget fails with BSAR_ERR_OOM_BUDGET; smaller
+ * ones wait. */
 bsar_status bsar_server_estimate(const bsar_request* req, uint64_t* bytes);
 /* done = 1 when the request finished; its status is the return value once done. */
 bsar_status bsar_server_poll(bsar_server* srv, bsar_request_id id, int32_t* done, double* latency_ms);
