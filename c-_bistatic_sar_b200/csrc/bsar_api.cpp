@@ -410,16 +410,6 @@ bsar_status bsar_scene_read_stored(bsar_ctx* ctx, bsar_scene_id id, int32_t prec
     });
 }
 
-static void check_grid(const bsar_grid* g)
-{
-    if (!g) fail(BSAR_ERR_INVALID_ARG, "grid is NULL");
-    if (g->nx < 1 || g->ny < 1 || g->nz < 1 || !g->x_axis || !g->y_axis || !g->z_axis)
-        fail(BSAR_ERR_INVALID_ARG, "empty grid");
-    if (g->nx * g->ny * g->nz > ((int64_t)1 << 34)) fail(BSAR_ERR_INVALID_ARG, "grid too large");
-    if (!all_finite(g->x_axis, g->nx) || !all_finite(g->y_axis, g->ny) || !all_finite(g->z_axis, g->nz))
-        fail(BSAR_ERR_INVALID_ARG, "non-finite grid axis");
-}
-
 // Stage the grid axes; reuse the device copy when the axes did not change.
 static const double* stage_grid(bsar_ctx* ctx, const bsar_grid* g)
 {
@@ -512,8 +502,7 @@ bsar_status bsar_backproject(bsar_ctx* ctx, bsar_scene_id id, const bsar_grid* g
 {
     return guarded(ctx, [&] {
         if (!image_out) fail(BSAR_ERR_INVALID_ARG, "image_out is NULL");
-        check_grid(g);
-        int64_t nv = g->nx * g->ny * g->nz;
+        const int64_t nv = check_grid(g);
         auto img = dev_alloc(ctx, sizeof(double2) * nv);
         backproject(ctx, id, g, o, img->as<double2>());
         cuda_check(cudaMemcpyAsync(image_out, img->p, sizeof(double2) * nv, cudaMemcpyDeviceToHost, ctx->stream), "d2h");

@@ -18,12 +18,16 @@
 //   (cleared every call); the same chunking as the allocating entry point, so both
 //   give the same image
 //
-// The array is 64 MiB, and every GPU on which the library is loaded holds it until the
-// process exits.  It is one per device and per process and keeps the previous call's
-// contents: calls that overlap in time on one device (two threads, two contexts, or an
-// earlier call's work still on another stream) race on it.  The first call on a device
-// looks the array up (cudaGetSymbolAddress with that device current) and may load the
-// module; make that first call before any stream capture.
+// The array is 64 MiB.  A device commits it when this file's module is loaded there:
+// under CUDA's default lazy module loading that is the first call on the device (its
+// cudaGetSymbolAddress), with CUDA_MODULE_LOADING=EAGER it is when the library's first
+// CUDA call initialises the device.  Either way the device holds it until the process
+// exits.  So that first call is the one moment this entry point asks the driver for
+// memory: make it before another allocator (a framework's caching allocator) reserves
+// the device's memory, and before any stream capture -- or set
+// CUDA_MODULE_LOADING=EAGER.  The array is one per device and per process and keeps
+// the previous call's contents: calls that overlap in time on one device (two threads,
+// two contexts, or an earlier call's work still on another stream) race on it.
 #include <mutex>
 
 #include "runtime.hpp"
@@ -53,15 +57,10 @@ size_t up256(size_t x) { return (x + 255) & ~size_t(255); }
 extern "C" bsar_status bsar_backproject_mixed_noalloc(bsar_ctx* ctx, bsar_scene_id id, const bsar_grid* g,
                                                       const bsar_bp_opts* o, double* image_out)
 {
-    if (!ctx) return BSAR_ERR_INVALID_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mu);
-    try {
-        cuda_check(cudaSetDevice(ctx->device), "cudaSetDevice");
-        if (!image_out || !g || !o) fail(BSAR_ERR_INVALID_ARG, "NULL argument");
-        if (g->nx < 1 || g->ny < 1 || g->nz < 1 || !g->x_axis || !g->y_axis || !g->z_axis)
-            fail(BSAR_ERR_INVALID_ARG, "empty grid");
-        if (!all_finite(g->x_axis, g->nx) || !all_finite(g->y_axis, g->ny) || !all_finite(g->z_axis, g->nz))
-            fail(BSAR_ERR_INVALID_ARG, "non-finite grid axis");
+    return guarded(ctx, [&] {
+        if (!image_out || !o) fail(BSAR_ERR_INVALID_ARG, "NULL argument");
+        // axes bounded one factor at a time: the voxel count below cannot wrap
+        const int64_t nv = check_grid(g);
         if (o->solver != BSAR_SOLVER_NEWTON || o->legs != BSAR_LEGS_PER_PULSE ||
             (o->precision != BSAR_MIXED && o->precision != BSAR_MIXED_FP16))
             fail(BSAR_ERR_UNSUPPORTED, "this entry point runs the mixed forms (Newton, per-pulse legs)");
@@ -72,7 +71,6 @@ extern "C" bsar_status bsar_backproject_mixed_noalloc(bsar_ctx* ctx, bsar_scene_
         if (!s->rc[o->precision].data)
             fail(BSAR_ERR_INVALID_ARG, "the scene has no samples for this precision: call bsar_scene_compress first");
         const int64_t np = s->np;
-        const int64_t nv = g->nx * g->ny * g->nz;
         // scratch layout and its limit
         const size_t o_req = 0;
         const size_t o_cnt = o_req + up256(sizeof(MixedReq));
@@ -173,10 +171,5 @@ extern "C" bsar_status bsar_backproject_mixed_noalloc(bsar_ctx* ctx, bsar_scene_
         cuda_check(cudaMemcpyAsync(&hstat, status, sizeof(int), cudaMemcpyDeviceToHost, st), "status");
         sync(ctx);
         if (hstat) fail(BSAR_ERR_TIMEOUT, "a device-side DEM tile copy did not complete within its wait limit");
-        clear_error(ctx);
-        return BSAR_OK;
-    } catch (const Error& e) {
-        set_error(ctx, e.msg);
-        return e.status;
-    }
+    });
 }

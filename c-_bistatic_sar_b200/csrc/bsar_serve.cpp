@@ -615,9 +615,12 @@ bsar_status bsar_server_submit(bsar_server* s, const bsar_request* q, bsar_reque
     const int64_t np = d.n_pulses;
     if (np < 1 || !d.tx || !d.rx || d.dem.nx < 2 || d.dem.ny < 2 || !d.dem.x_vec || !d.dem.y_vec || !d.dem.z)
         return BSAR_ERR_INVALID_ARG;
-    if (q->grid.nx < 1 || q->grid.ny < 1 || q->grid.nz < 1 || !q->grid.x_axis || !q->grid.y_axis || !q->grid.z_axis ||
-        !q->image_out)
+    if (!q->image_out) return BSAR_ERR_INVALID_ARG;
+    try {
+        check_grid(&q->grid);          // sizes bounded before any product is formed
+    } catch (const Error&) {
         return BSAR_ERR_INVALID_ARG;
+    }
     if (q->opts.solver != BSAR_SOLVER_NEWTON || q->opts.legs != BSAR_LEGS_PER_PULSE ||
         (q->opts.precision != BSAR_MIXED && q->opts.precision != BSAR_MIXED_FP16))
         return BSAR_ERR_UNSUPPORTED;

@@ -997,18 +997,26 @@ int mixed_chunks(int64_t voxels, int pulses)
     return (int)k;
 }
 
+// Resident CTAs of the current device, looked up once per device: the pulse-chunk count
+// (and with it a small grid's summation order) follows the device the call runs on, so
+// GPUs of different kinds in one process each get their own.
 int mixed_grid_ctas()
 {
     mixed_setup_device();
-    static int ctas = 0;
-    if (!ctas) {
-        int dev = 0, sms = 148, per = 0;
-        cudaGetDevice(&dev);
+    constexpr int kDevs = 64;
+    static std::atomic<int> ctas[kDevs];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::atomic<int>* slot = (dev >= 0 && dev < kDevs) ? &ctas[dev] : nullptr;
+    int n = slot ? slot->load() : 0;
+    if (!n) {
+        int sms = 148, per = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_bp_mixed<6, false>, 128, 0);
-        ctas = sms * (per > 0 ? per : 1);
+        n = sms * (per > 0 ? per : 1);
+        if (slot) slot->store(n);
     }
-    return ctas;
+    return n;
 }
 
 template <bool CH> static void launch_w(const MixedBatch& b, int W, int grid, cudaStream_t st)

@@ -430,6 +430,27 @@ inline bool all_finite(const double* p, int64_t n)
     return true;
 }
 
+// Largest imaging grid (voxels) a call takes.
+constexpr int64_t kMaxGridVoxels = (int64_t)1 << 34;
+
+// Checks an imaging grid and returns its voxel count.  Every axis must fit an int (the
+// kernels index axes with 32-bit integers) and the product is bounded one factor at a
+// time, so nx * ny * nz cannot wrap.
+inline int64_t check_grid(const bsar_grid* g)
+{
+    if (!g) fail(BSAR_ERR_INVALID_ARG, "grid is NULL");
+    if (g->nx < 1 || g->ny < 1 || g->nz < 1 || !g->x_axis || !g->y_axis || !g->z_axis)
+        fail(BSAR_ERR_INVALID_ARG, "empty grid");
+    constexpr int64_t kMaxAxis = 0x7fffffff;
+    if (g->nx > kMaxAxis || g->ny > kMaxAxis || g->nz > kMaxAxis || g->nx > kMaxGridVoxels / g->ny ||
+        g->nx * g->ny > kMaxGridVoxels / g->nz)
+        fail(BSAR_ERR_INVALID_ARG, "grid too large (%lld x %lld x %lld voxels; at most 2^34)", (long long)g->nx,
+             (long long)g->ny, (long long)g->nz);
+    if (!all_finite(g->x_axis, g->nx) || !all_finite(g->y_axis, g->ny) || !all_finite(g->z_axis, g->nz))
+        fail(BSAR_ERR_INVALID_ARG, "non-finite grid axis");
+    return g->nx * g->ny * g->nz;
+}
+
 // createCHIRP (src/raw_data_processing.cpp:257-290) and the fftshifted reference
 // (:371-394) of length n.
 inline std::vector<double> matched_reference(double f0, double f1, double T, double fs, int64_t n)

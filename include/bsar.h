@@ -252,11 +252,15 @@ bsar_status bsar_backproject_device(bsar_ctx* ctx, bsar_scene_id scene, const bs
  * where a cudaMalloc fails or makes that allocator release memory, and latency-critical
  * loops that cannot take the device-wide wait of a cudaFree.  Request record, work
  * counter, status word, anchors, grid axes and image live in one fixed 64 MiB scratch
- * array per device, held from library load to process exit (a call that does not fit,
- * beyond about 4M voxels, fails with BSAR_ERR_INVALID_ARG).  The scene must already hold
- * samples for the precision (bsar_scene_compress).  Calls that overlap in time on one
- * device race on the scratch.  The first call on a device sets the scratch up; make it
- * before any stream capture. */
+ * array per device (a call that does not fit, beyond about 4M voxels, fails with
+ * BSAR_ERR_INVALID_ARG).  The device commits the array when the module holding it
+ * loads -- under CUDA's default lazy loading at the first call on that device, with
+ * CUDA_MODULE_LOADING=EAGER at the library's first CUDA call -- and holds it until the
+ * process exits.  That first call is therefore the one moment memory is taken: make it
+ * before another allocator reserves the device's memory and before any stream capture,
+ * or set CUDA_MODULE_LOADING=EAGER.  The scene must already hold samples for the
+ * precision (bsar_scene_compress).  Calls that overlap in time on one device race on the
+ * scratch. */
 bsar_status bsar_backproject_mixed_noalloc(bsar_ctx* ctx, bsar_scene_id scene, const bsar_grid* grid,
                                            const bsar_bp_opts* opts, double* image_out);
 

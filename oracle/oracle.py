@@ -23,7 +23,9 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ORACLE_SO = HERE / "libbsar_oracle.so"
 REF_SO = HERE / "_ref" / "libbsar_ref.so"
-REF_TREE = Path(os.environ.get("BSAR_REFERENCE_TREE", "/root/reference"))
+# the reference checkout: $BSAR_REFERENCE_TREE, else a `reference` directory beside the
+# repository
+REF_TREE = Path(os.environ.get("BSAR_REFERENCE_TREE", str(HERE.parent.parent / "reference")))
 
 _d = C.POINTER(C.c_double)
 _i64 = C.c_int64

@@ -6,7 +6,6 @@ equal the reference's.
 GPU: the driver runs and its results equal the oracle's (bit-exact Fermat, DEM and spline;
 FFTs to 1e-12), including the reference's non-power-of-two FFT behaviour.
 """
-import os
 import subprocess
 from pathlib import Path
 
@@ -19,7 +18,7 @@ import oracle as O
 ROOT = Path(__file__).resolve().parent.parent
 LIB = ROOT / "c-_bistatic_sar_b200" / "lib"
 DRIVER = ROOT / "tests" / "compat" / "compat_driver.cpp"
-REF_INC = Path(os.environ.get("BSAR_REFERENCE_TREE", "/root/reference")) / "include"
+REF_INC = O.REF_TREE / "include"
 
 
 def _build(out: Path, use_bsar_header: bool):

@@ -24,6 +24,12 @@ def chunked_scene():
                                  dz=0.1, n_scatterers=4))
 
 
+def _device_free_bytes() -> int:
+    """cudaMemGetInfo's free bytes of device 0 (the driver's view, not a pool's)."""
+    import torch
+    return int(torch.cuda.mem_get_info(0)[0])
+
+
 def _alloc(ctx, sid, gx, gy, gz, precision):
     return ctx.backproject(sid, gx, gy, gz, solver="newton", legs="per_pulse", precision=precision)
 
@@ -38,8 +44,13 @@ def test_noalloc_matches_allocating_entry_point(ctx, which, precision, request):
         ref = _alloc(ctx, sid, scene.gx, scene.gy, scene.gz, precision)
         used = ctx.bytes_in_use
         first = ctx.backproject_mixed_noalloc(sid, scene.gx, scene.gy, scene.gz, precision=precision)
+        # the first call may load the scratch's module; after it the device's free memory
+        # must not move (an allocation outside the context's pool would show here)
+        free_before = _device_free_bytes()
         second = ctx.backproject_mixed_noalloc(sid, scene.gx, scene.gy, scene.gz, precision=precision)
+        free_after = _device_free_bytes()
         assert ctx.bytes_in_use == used
+        assert abs(free_after - free_before) < (1 << 20), (free_before, free_after)
     finally:
         ctx.scene_release(sid)
     assert np.array_equal(first, ref)
