@@ -27,6 +27,7 @@ STATUS = {0: "ok", 1: "invalid argument", 2: "HBM budget exceeded", 3: "device w
 SOLVER = {"grid": 0, "newton": 1}
 LEGS = {"mean": 0, "per_pulse": 1}
 PRECISION = {"fp64": 0, "mixed": 1, "mixed_fp16": 2}
+EXHAUSTIVE = 1   # BSAR_BP_EXHAUSTIVE_SCAN
 FILE_LAYOUT = {"as_imager": 0, "row_major": 1}
 
 
@@ -366,11 +367,14 @@ class Context:
         return (gx, gy, gz), Grid(len(gx), len(gy), len(gz), _p(gx), _p(gy), _p(gz))
 
     def backproject(self, sid: int, gx, gy, gz, *, solver="grid", legs="mean", precision="fp64",
-                    search_radius_m=0.0, out=None):
+                    search_radius_m=0.0, out=None, exhaustive=False):
         """Image [x][y][z] complex128; `out` (C-contiguous complex128 of that shape, e.g.
-        a view of pinned memory) receives it instead of a new array."""
+        a view of pinned memory) receives it instead of a new array.  `exhaustive`: the
+        mixed forms rank every node of each node-scan window (BSAR_BP_EXHAUSTIVE_SCAN;
+        the same image, slower)."""
         keep, g = self._grid(gx, gy, gz)
-        o = BpOpts(SOLVER[solver], LEGS[legs], PRECISION[precision], 0, search_radius_m)
+        o = BpOpts(SOLVER[solver], LEGS[legs], PRECISION[precision], EXHAUSTIVE if exhaustive else 0,
+                   search_radius_m)
         if out is None:
             out = np.empty((g.nx, g.ny, g.nz), dtype=np.complex128)
         elif out.shape != (g.nx, g.ny, g.nz) or out.dtype != np.complex128 or not out.flags.c_contiguous:
@@ -378,20 +382,23 @@ class Context:
         self._ok(self.L.bsar_backproject(self.h, sid, C.byref(g), C.byref(o), _p(out.view(np.float64))))
         return out
 
-    def backproject_mixed_noalloc(self, sid: int, gx, gy, gz, *, precision="mixed", search_radius_m=0.0):
+    def backproject_mixed_noalloc(self, sid: int, gx, gy, gz, *, precision="mixed", search_radius_m=0.0,
+                                  exhaustive=False):
         """Mixed back-projection that allocates no GPU memory, for callers whose GPU memory
         belongs to another allocator: a fixed 64 MiB per-device scratch, one call at a
         time per device; the scene must already be compressed for `precision`."""
         keep, g = self._grid(gx, gy, gz)
-        o = BpOpts(SOLVER["newton"], LEGS["per_pulse"], PRECISION[precision], 0, search_radius_m)
+        o = BpOpts(SOLVER["newton"], LEGS["per_pulse"], PRECISION[precision], EXHAUSTIVE if exhaustive else 0,
+                   search_radius_m)
         out = np.empty((g.nx, g.ny, g.nz), dtype=np.complex128)
         self._ok(self.L.bsar_backproject_mixed_noalloc(self.h, sid, C.byref(g), C.byref(o), _p(out.view(np.float64))))
         return out
 
     def backproject_device(self, sid: int, gx, gy, gz, d_image_ptr: int, *, solver="grid", legs="mean",
-                           precision="fp64", search_radius_m=0.0):
+                           precision="fp64", search_radius_m=0.0, exhaustive=False):
         keep, g = self._grid(gx, gy, gz)
-        o = BpOpts(SOLVER[solver], LEGS[legs], PRECISION[precision], 0, search_radius_m)
+        o = BpOpts(SOLVER[solver], LEGS[legs], PRECISION[precision], EXHAUSTIVE if exhaustive else 0,
+                   search_radius_m)
         self._ok(self.L.bsar_backproject_device(self.h, sid, C.byref(g), C.byref(o), C.c_void_p(d_image_ptr)))
 
 
@@ -419,7 +426,7 @@ def upload_scene(ctx: Context, scene, kind="raw") -> int:
 
 def _request(dem: DemArrays, tx, rx, gx, gy, gz, *, samples=None, n_samples=None, kind="raw", scat_pos=None,
              scat_amp=None, snr_db=float("inf"), seed=0, upsample=4, n1=1.0, n2=2.0, c=3e8, fc=1e9, fs=1.2e9,
-             chirp_f0=0.0, chirp_f1=0.0, chirp_T=0.0, precision="mixed", search_radius_m=0.0):
+             chirp_f0=0.0, chirp_f1=0.0, chirp_T=0.0, precision="mixed", search_radius_m=0.0, exhaustive=False):
     """bsar_request for the server, the output image and the arrays the request points into."""
     tx = _f64(tx, (-1, 3))
     rx = _f64(rx, (-1, 3))
@@ -441,7 +448,8 @@ def _request(dem: DemArrays, tx, rx, gx, gy, gz, *, samples=None, n_samples=None
     axes, g = Context._grid(gx, gy, gz)
     keep.append(axes)
     out = np.empty((g.nx, g.ny, g.nz), dtype=np.complex128)
-    o = BpOpts(SOLVER["newton"], LEGS["per_pulse"], PRECISION[precision], 0, search_radius_m)
+    o = BpOpts(SOLVER["newton"], LEGS["per_pulse"], PRECISION[precision], EXHAUSTIVE if exhaustive else 0,
+               search_radius_m)
     req = Request(desc, _p(pos), _p(amp), nscat, snr_db, seed & (2**64 - 1), g, o, _p(out.view(np.float64)))
     return req, out, keep
 

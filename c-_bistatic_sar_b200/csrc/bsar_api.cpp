@@ -435,6 +435,7 @@ static void backproject(bsar_ctx* ctx, bsar_scene_id id, const bsar_grid* g, con
     if (o->solver != BSAR_SOLVER_GRID && o->solver != BSAR_SOLVER_NEWTON) fail(BSAR_ERR_INVALID_ARG, "unknown solver");
     if (o->legs != BSAR_LEGS_MEAN && o->legs != BSAR_LEGS_PER_PULSE) fail(BSAR_ERR_INVALID_ARG, "unknown legs mode");
     if (o->precision < BSAR_FP64 || o->precision > BSAR_MIXED_FP16) fail(BSAR_ERR_INVALID_ARG, "unknown precision");
+    if (o->flags & ~BSAR_BP_EXHAUSTIVE_SCAN) fail(BSAR_ERR_INVALID_ARG, "unknown back-projection flags");
     if (o->precision != BSAR_FP64 && o->solver != BSAR_SOLVER_NEWTON)
         fail(BSAR_ERR_UNSUPPORTED, "the mixed forms use the Newton solver");
     if (o->precision != BSAR_FP64 && o->legs != BSAR_LEGS_PER_PULSE)
@@ -476,7 +477,7 @@ static void backproject(bsar_ctx* ctx, bsar_scene_id id, const bsar_grid* g, con
     set_anchors(ctx, s, g, a);
     if (o->legs != BSAR_LEGS_PER_PULSE) fail(BSAR_ERR_UNSUPPORTED, "the mixed forms use per-pulse legs");
     ensure_mixed_buffers(ctx);
-    MixedReq r = mixed_request(s, a, o->precision == BSAR_MIXED_FP16);
+    MixedReq r = mixed_request(s, a, o->precision == BSAR_MIXED_FP16, o->flags);
     // small grids: each tile's pulses in K chunks, so the work items fill the GPU
     const int64_t vtiles = (a.v_count + 127) / 128;
     const int K = mixed_chunks(a.v_count, a.np);

@@ -61,6 +61,7 @@ extern "C" bsar_status bsar_backproject_mixed_noalloc(bsar_ctx* ctx, bsar_scene_
         if (!image_out || !o) fail(BSAR_ERR_INVALID_ARG, "NULL argument");
         // axes bounded one factor at a time: the voxel count below cannot wrap
         const int64_t nv = check_grid(g);
+        if (o->flags & ~BSAR_BP_EXHAUSTIVE_SCAN) fail(BSAR_ERR_INVALID_ARG, "unknown back-projection flags");
         if (o->solver != BSAR_SOLVER_NEWTON || o->legs != BSAR_LEGS_PER_PULSE ||
             (o->precision != BSAR_MIXED && o->precision != BSAR_MIXED_FP16))
             fail(BSAR_ERR_UNSUPPORTED, "this entry point runs the mixed forms (Newton, per-pulse legs)");
@@ -151,7 +152,7 @@ extern "C" bsar_status bsar_backproject_mixed_noalloc(bsar_ctx* ctx, bsar_scene_
                 }
             }
         }
-        MixedReq r = mixed_request(s, a, o->precision == BSAR_MIXED_FP16);
+        MixedReq r = mixed_request(s, a, o->precision == BSAR_MIXED_FP16, o->flags);
         r.off_x = (float)(ox / (2.0 * np));
         r.off_y = (float)(oy / (2.0 * np));
         MixedChunks* d_chunks = nullptr;

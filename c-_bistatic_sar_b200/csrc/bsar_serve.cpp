@@ -246,7 +246,7 @@ void admit(bsar_server* s, Req* r)
         g.z_axis = r->gz.data();
         set_anchors(ctx, sc, &g, a);
         sync(ctx);
-        r->rec = mixed_request(sc, a, r->opts.precision == BSAR_MIXED_FP16);
+        r->rec = mixed_request(sc, a, r->opts.precision == BSAR_MIXED_FP16, r->opts.flags);
         if (K > 1) r->chunks = MixedChunks{K, 0, r->partial->as<double2>(), r->tile_done->as<int>()};
         r->ntiles = vtiles * K;             // work items: (tile, chunk) pairs
         r->voxel_pulses = (double)nv * (double)sc->np;
@@ -621,6 +621,7 @@ bsar_status bsar_server_submit(bsar_server* s, const bsar_request* q, bsar_reque
     } catch (const Error&) {
         return BSAR_ERR_INVALID_ARG;
     }
+    if (q->opts.flags & ~BSAR_BP_EXHAUSTIVE_SCAN) return BSAR_ERR_INVALID_ARG;
     if (q->opts.solver != BSAR_SOLVER_NEWTON || q->opts.legs != BSAR_LEGS_PER_PULSE ||
         (q->opts.precision != BSAR_MIXED && q->opts.precision != BSAR_MIXED_FP16))
         return BSAR_ERR_UNSUPPORTED;

@@ -66,6 +66,7 @@ struct MixedCtx {
     double ox, oy;                  // origin of the FP32 frame (first DEM node)
     double idx64, idy64;            // 1 / spacing, FP64
     float start_band;               // node units: FP32 starts this close to a cell boundary go FP64
+    int prune;                      // node scans may skip what the lower bound excludes
 };
 
 // Start heights under a voxel (the lower endpoint of both of its paths when the ground
@@ -308,34 +309,57 @@ template <int WT> struct TableRows { static constexpr int v = WT > 0 ? 2 * WT + 
 
 struct AirTable {
     float2* t;
+    float* rowz;        // lowest height of each table row (over the table's columns)
     int i0, j0;
+    float zmin;         // lowest height of the whole table
     bool ok;
 };
 
+// Float <-> unsigned key with the same order (for the warp min reduction of heights).
+__device__ __forceinline__ unsigned order_key(float f)
+{
+    const unsigned u = __float_as_uint(f);
+    return (u >> 31) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float order_key_float(unsigned k)
+{
+    return __uint_as_float((k >> 31) ? (k & 0x7fffffffu) : ~k);
+}
+
 template <int TBI>
-__device__ __forceinline__ AirTable build_air_table(const MixedCtx& m, const Tile& T, float2* buf, int is, int js, int W,
-                                                    float ex, float ey, float ez, float re)
+__device__ __forceinline__ AirTable build_air_table(const MixedCtx& m, const Tile& T, float2* buf, float* rowz, int is,
+                                                    int js, int W, float ex, float ey, float ez, float re)
 {
     const unsigned full = 0xffffffffu;
     int i0 = max(__reduce_min_sync(full, is) - W, 0), i1 = min(__reduce_max_sync(full, is) + W, m.nx - 1);
     int j0 = max(__reduce_min_sync(full, js) - W, 0), j1 = min(__reduce_max_sync(full, js) + W, m.ny - 1);
-    AirTable A{buf, i0, j0, false};
+    AirTable A{buf, rowz, i0, j0, INFINITY, false};
     __syncwarp();                       // readers of the previous table are done
     if (i1 - i0 + 1 > TBI || j1 - j0 + 1 > TBJ) return A;
     const int lane = threadIdx.x & 31;
     const int j = j0 + lane;
+    const bool col = j <= j1;
     const bool in_tile = T.ok && i0 >= T.i0 && i1 < T.i0 + TI && j0 >= T.j0 && j1 < T.j0 + TJ;
-    if (j <= j1) {
-        float dy = (float)j * m.stepy - ey;
-        float sy = dy * dy;
-        for (int i = i0; i <= i1; i++) {
+    float dy = (float)j * m.stepy - ey;
+    float sy = dy * dy;
+    unsigned kmin = 0xffffffffu;
+    // every lane walks the rows (the row minimum is a warp reduction); lanes right of the
+    // union's last column only take part in it
+    for (int i = i0; i <= i1; i++) {
+        unsigned key = 0xffffffffu;
+        if (col) {
             float z = in_tile ? T.s[(j - T.j0) * TI + (i - T.i0)] : zf(m, i, j);
             float dx = (float)i * m.stepx - ex, dz = z - ez;
             float q = fmaf(dz, dz, fmaf(dx, dx, sy));
             buf[(i - i0) * TBJ + lane] = make_float2(z, re * (q * rsqrtf(q)));
+            key = order_key(z);
         }
+        const unsigned rk = __reduce_min_sync(full, key);
+        kmin = min(kmin, rk);
+        if (lane == 0) rowz[i - i0] = order_key_float(rk);
     }
     __syncwarp();
+    A.zmin = order_key_float(kmin);
     A.ok = true;
     return A;
 }
@@ -379,16 +403,153 @@ __device__ __forceinline__ void scan_table(const MixedCtx& m, const AirTable& AT
     bj = js - W + bc;
 }
 
+// Columns of a window row in groups of four for the pruned scan; a trailing single column
+// joins the last group (13 columns: 0-3, 4-7, 8-12).
+template <int W> struct ColGroups {
+    static constexpr int NJ = 2 * W + 1;
+    static constexpr int N = (NJ % 4 == 1) ? NJ / 4 : (NJ + 3) / 4;
+    __host__ __device__ static constexpr int first(int k) { return 4 * k; }
+    __host__ __device__ static constexpr int last(int k) { return k == N - 1 ? NJ - 1 : 4 * k + 3; }
+};
+
+// The table scan with exact pruning: rows, and groups of columns inside a row, whose
+// ranking values provably all exceed the pruning threshold are skipped.  The result (best
+// value, best node, and whether the runner-up lies within the tie band) is that of
+// scan_table, bit for bit:
+//  * a skipped node's value exceeds v1 + tie at the time of the skip, so it is neither the
+//    minimum nor within the tie band of the final minimum, and v2 - v1 >= tie is decided
+//    as before;
+//  * an exact FP32 tie between two nodes puts v2 == v1 and sends the lane to the FP64
+//    re-rank, so the order in which rows are visited (centre outward) does not choose
+//    between equal values.
+// The bound.  The E leg e(N) = re |N - E| is convex, so it lies above its tangent plane
+// at the start node N0: e(N) >= K + a.(N - G), a = re (N0 - E) / |N0 - E|.  On a row
+// (x fixed) with every height above zlo, the ranking value is at least
+//     K + a_x X + a_z Zl + min_Y [a_y Y + sqrt(X^2 + Zl^2 + Y^2)]
+// (X, Y, Zl: offsets from the voxel G; Zl from the row's lowest height), valid while
+// a_z Z + |N - G| grows with the height Z over the window (checked once per solve).  With
+// t = thr - K - a_x X - a_z Zl, the row holds no node at or below thr when t < 0 or
+// t^2 < (1 - a_y^2)(X^2 + Zl^2); a column group, whose Y lies in [Ylo, Yhi] and whose own
+// lowest height gives Zl, holds none when t < 0 or the parabola
+// (1 - a_y^2) Y^2 + 2 t a_y Y + X^2 + Zl^2 - t^2 is positive on [Ylo, Yhi].  The
+// threshold is v1 + tie, or sooner the value of `seed` (the previous pulse's best node,
+// when it lies in this window) + tie, widened by a margin far above the FP32 rounding of
+// the values and of the bound.  Warp-uniform: a row or group is skipped only when no lane
+// of the warp needs it, so all 32 lanes must call together.
+template <int W>
+__device__ __forceinline__ void scan_pruned(const MixedCtx& m, const AirTable& AT, int is, int js, const float E[3],
+                                            float gx, float gy, float gz, float re, float tie, int seed, float& v1,
+                                            float& v2, int& bi, int& bj)
+{
+    using CG = ColGroups<W>;
+    constexpr int NJ = 2 * W + 1;
+    const unsigned full = 0xffffffffu;
+    float syg[NJ];
+#pragma unroll
+    for (int c = 0; c < NJ; c++) {
+        float dy = (float)(js - W + c) * m.stepy - gy;
+        syg[c] = dy * dy;
+    }
+    const float2* row0 = AT.t + (is - W - AT.i0) * TBJ + (js - W - AT.j0);
+    // tangent plane of the E leg at the start node N0
+    const float2 n0 = row0[W * TBJ + W];
+    const float x0 = (float)is * m.stepx, y0 = (float)js * m.stepy;
+    const float kk = re * re / n0.y;                    // re / |N0 - E|
+    const float ax = (x0 - E[0]) * kk, ay = (y0 - E[1]) * kk, az = (n0.x - E[2]) * kk;
+    const float K = n0.y + ax * (gx - x0) + ay * (gy - y0) + az * (gz - n0.x);
+    const float sy2 = 1.0f - ay * ay;
+    const float yv_t = -ay / sy2;                       // vertex of the parabola: Y = t * yv_t
+    const float ay2 = 2.0f * ay;
+    const float yfirst = (float)(js - W) * m.stepy - gy;
+    // height monotonicity over the window (else nothing is pruned)
+    const float Zt = AT.zmin - gz;
+    const float hx = fabsf(x0 - gx) + (float)W * m.stepx, hy = fabsf(y0 - gy) + (float)W * m.stepy;
+    const bool bound_ok = sy2 > 1e-3f &&           // |a| = re: the bound needs the E leg's index below the G leg's
+                          (az >= 0.0f || (Zt > 0.0f && az * az * (hx * hx + hy * hy + Zt * Zt) <= Zt * Zt));
+    // seed: the previous pulse's best node, ranked with the scan's own arithmetic
+    float thr_seed = INFINITY;
+    {
+        const int si = seed >> 16, sj = seed & 0xffff;
+        if (seed >= 0 && abs(si - is) <= W && abs(sj - js) <= W) {
+            const float2 e = row0[(si - is + W) * TBJ + (sj - js + W)];
+            const float dx = (float)si * m.stepx - gx, dy = (float)sj * m.stepy - gy;
+            const float dz = e.x - gz;
+            const float q = fmaf(dz, dz, dx * dx + dy * dy);
+            thr_seed = fmaf(q, rsqrtf(q), e.y);
+        }
+    }
+    const float never = bound_ok ? 0.0f : INFINITY;     // +inf: keep every row
+    int bc = bj - (js - W);
+#pragma unroll 1
+    for (int k = 0; k < NJ; k++) {
+        const int d = (k + 1) >> 1;
+        const int r = (k & 1) ? W - d : W + d;          // rows from the start node outward
+        const int i = is - W + r;
+        const float dx = (float)i * m.stepx - gx;
+        const float sxg = dx * dx;
+        const float2* row = row0 + r * TBJ;
+        const float v1_row = v1;
+        float T = fminf(thr_seed, v1) + tie + never;
+        T = T + fmaf(4e-6f, fabsf(T), 2e-4f);
+        const float R = T - K - ax * dx;
+        {
+            const float zl = AT.rowz[i - AT.i0] - gz;
+            const float t = R - az * zl;
+            const bool skip = t < 0.0f || t * t < sy2 * fmaf(zl, zl, sxg);
+            if (!__any_sync(full, !skip)) continue;
+        }
+#pragma unroll
+        for (int g = 0; g < CG::N; g++) {
+            const int c0 = CG::first(g), c1 = CG::last(g);
+            float2 e[5];
+            float zc = INFINITY;
+#pragma unroll
+            for (int c = 0; c < 5; c++)
+                if (c0 + c <= c1) {
+                    e[c] = row[c0 + c];
+                    zc = fminf(zc, e[c].x);
+                }
+            const float zl = zc - gz;
+            const float t = R - az * zl;
+            const float ylo = fmaf((float)c0, m.stepy, yfirst), yhi = fmaf((float)c1, m.stepy, yfirst);
+            const float yc = fminf(fmaxf(t * yv_t, ylo), yhi);
+            const float q = fmaf(fmaf(sy2, yc, ay2 * t), yc, fmaf(-t, t, fmaf(zl, zl, sxg)));
+            const bool skip = t < 0.0f || q > 0.0f;
+            if (!__any_sync(full, !skip)) continue;
+#pragma unroll
+            for (int c = 0; c < 5; c++)
+                if (c0 + c <= c1) {
+                    const float dz = e[c].x - gz;
+                    const float qq = fmaf(dz, dz, sxg + syg[c0 + c]);
+                    const float L = fmaf(qq, rsqrtf(qq), e[c].y);
+                    v2 = fminf(v2, fmaxf(v1, L));
+                    const bool p = L < v1;
+                    v1 = p ? L : v1;
+                    bc = p ? c0 + c : bc;
+                }
+        }
+        bi = (v1 < v1_row) ? i : bi;
+    }
+    bj = js - W + bc;
+}
+
 template <int W, bool TABLE>
 __device__ __forceinline__ void node_scan(const MixedCtx& m, const Tile& T, const AirTable& AT, int is, int js, int Wr,
-                                          const float E[3], const float G[3], float re, float& v1, float& v2, int& bi,
-                                          int& bj)
+                                          const float E[3], const float G[3], float re, float tie, int seed, float& v1,
+                                          float& v2, int& bi, int& bj)
 {
     const int ia = max(is - Wr, 0), ib = min(is + Wr, m.nx - 1);
     const int ja = max(js - Wr, 0), jb = min(js + Wr, m.ny - 1);
     const bool in_tile = T.ok && ia >= T.i0 && ib < T.i0 + TI && ja >= T.j0 && jb < T.j0 + TJ;
     if constexpr (W > 0 && TABLE) {
-        if (AT.ok && Wr == W && ia == is - W && ib == is + W && ja == js - W && jb == js + W) {
+        const bool full_window = AT.ok && Wr == W && ia == is - W && ib == is + W && ja == js - W && jb == js + W;
+        // the pruned scan votes across the warp: only when every lane takes it
+        const bool all_full = __all_sync(0xffffffffu, full_window);
+        if (all_full && m.prune) {
+            scan_pruned<W>(m, AT, is, js, E, G[0], G[1], G[2], re, tie, seed, v1, v2, bi, bj);
+            return;
+        }
+        if (full_window) {
             scan_table<W>(m, AT, is, js, G[0], G[1], G[2], v1, v2, bi, bj);
             return;
         }
@@ -514,11 +675,14 @@ __device__ __noinline__ int2 start_node64(const DemView d, double Ax, double Ay,
 // is B when g_is_b, else A.  A32/B32: the endpoints in the FP32 frame.  With TABLE the
 // warp builds and uses the shared E-leg table (all 32 lanes must call together).
 // Returns the FP64 optical path; dA, dB: FP64 leg lengths; X (optional): the crossing.
+// seed (table form): in, the node this lane chose for the same leg at the previous pulse
+// ((i << 16) | j, or -1), which only speeds up the pruned scan; out, the node chosen now.
 template <int WT, bool TABLE>
 __device__ __forceinline__ double solve_mixed(const DemView& d, const MixedCtx& m, const Tile& T, float2* table_buf,
-                                              const double A[3], const double B[3], const float A32[3],
-                                              const float B32[3], float na, float nb, bool g_is_b, int W,
-                                              const VoxelStart& vs, double& dA, double& dB, double* X = nullptr)
+                                              float* rowz_buf, const double A[3], const double B[3],
+                                              const float A32[3], const float B32[3], float na, float nb,
+                                              bool g_is_b, int W, const VoxelStart& vs, int& seed, double& dA,
+                                              double& dB, double* X = nullptr)
 {
     // 1. flat-interface start (FP32); the lower endpoint is normally the voxel itself
     const bool lower_b = nb >= na;
@@ -562,13 +726,13 @@ __device__ __forceinline__ double solve_mixed(const DemView& d, const MixedCtx& 
     const float* G = g_is_b ? B32 : A32;
     const float ng = g_is_b ? nb : na;
     const float re = (g_is_b ? na : nb) / ng;
-    AirTable AT{table_buf, 0, 0, false};
+    AirTable AT{table_buf, rowz_buf, 0, 0, INFINITY, false};
     if constexpr (TABLE && WT > 0)
-        AT = build_air_table<TableRows<WT>::v>(m, T, table_buf, is, js, W, E[0], E[1], E[2], re);
+        AT = build_air_table<TableRows<WT>::v>(m, T, table_buf, rowz_buf, is, js, W, E[0], E[1], E[2], re);
     float v1 = INFINITY, v2 = INFINITY;
     int bi = is, bj = js;
-    node_scan<WT, TABLE>(m, T, AT, is, js, W, E, G, re, v1, v2, bi, bj);
     const float tie = kTieM / ng;
+    node_scan<WT, TABLE>(m, T, AT, is, js, W, E, G, re, tie, seed, v1, v2, bi, bj);
     const bool need = !(v2 - v1 >= tie);
     if constexpr (TABLE) {
         if (__any_sync(0xffffffffu, need)) {
@@ -585,6 +749,7 @@ __device__ __forceinline__ double solve_mixed(const DemView& d, const MixedCtx& 
         bi = b.x;
         bj = b.y;
     }
+    seed = (bi < 32768 && bj < 65536) ? (bi << 16) | bj : -1;
     // 3. polish the facets around the best node (FP32); heights from the DEM tile when the
     //    node's 3 x 3 neighbourhood lies in it
     const bool nt = T.ok && bi - 1 >= T.i0 && bi + 1 < T.i0 + TI && bj - 1 >= T.j0 && bj + 1 < T.j0 + TJ;
@@ -701,6 +866,7 @@ __device__ __forceinline__ MixedCtx req_ctx(const MixedReq& r)
     m.idx64 = r.idx64;
     m.idy64 = r.idy64;
     m.start_band = r.start_band;
+    m.prune = !r.exhaustive;
     return m;
 }
 
@@ -709,7 +875,8 @@ __device__ __forceinline__ MixedCtx req_ctx(const MixedReq& r)
 // The sum goes to dst at the voxel's image index.
 template <int WT, bool CH>
 __device__ __forceinline__ void voxel_mixed(const BpArgs& a, const MixedCtx& m, const Tile& T, float2* table_buf,
-                                            bool fp16, int64_t kk, int p0, int p1, double2* __restrict__ dst)
+                                            float* rowz_buf, bool fp16, int64_t kk, int p0, int p1,
+                                            double2* __restrict__ dst)
 {
     const int np = CH ? p1 : a.np;
     const float k_bin = (float)(a.fs_eff / a.c);
@@ -725,6 +892,7 @@ __device__ __forceinline__ void voxel_mixed(const BpArgs& a, const MixedCtx& m, 
     const float P32[3] = {(float)(P[0] - m.ox), (float)(P[1] - m.oy), (float)P[2]};
     const VoxelStart vs{height32(m, P32[0], P32[1]), dem_elevation(a.dem, P[0], P[1])};
     float accr = 0.f, acci = 0.f, cmpr = 0.f, cmpi = 0.f;
+    int seed0 = -1, seed1 = -1;     // each leg's node at the previous pulse (pruning hint)
     for (int i = CH ? p0 : 0; i < np; i++) {
         const double Tx[3] = {__ldg(a.tx + 3 * i), __ldg(a.tx + 3 * i + 1), __ldg(a.tx + 3 * i + 2)};
         const double Rx[3] = {__ldg(a.rx + 3 * i), __ldg(a.rx + 3 * i + 1), __ldg(a.rx + 3 * i + 2)};
@@ -741,8 +909,11 @@ __device__ __forceinline__ void voxel_mixed(const BpArgs& a, const MixedCtx& m, 
             const float A32[3] = {leg ? P32[0] : T32[0], leg ? P32[1] : T32[1], leg ? P32[2] : T32[2]};
             const float B32[3] = {leg ? R32[0] : P32[0], leg ? R32[1] : P32[1], leg ? R32[2] : P32[2]};
             double dA, dB;
-            L += solve_mixed<WT, true>(a.dem, m, T, table_buf, A, B, A32, B32, leg ? n2f : n1f, leg ? n1f : n2f,
-                                       leg == 0, a.W, vs, dA, dB);
+            int seed = leg ? seed1 : seed0;
+            L += solve_mixed<WT, true>(a.dem, m, T, table_buf, rowz_buf, A, B, A32, B32, leg ? n2f : n1f,
+                                       leg ? n1f : n2f, leg == 0, a.W, vs, seed, dA, dB);
+            seed1 = leg ? seed : seed1;
+            seed0 = leg ? seed0 : seed;
         }
         const float dL = (float)(L - __ldg(a.ref_L + i));
         // fast-time bin: integer anchor + FP32 offset
@@ -838,10 +1009,12 @@ __global__ void __launch_bounds__(128, 4) k_bp_mixed(MixedBatch b)
 {
     __shared__ alignas(128) float tile_s[TI * TJ];
     __shared__ alignas(16) float2 air_s[4][TableRows<WT>::v * TBJ];   // one (z, E-leg) table per warp
+    __shared__ float rowz_s[4][TableRows<WT>::v];                        // its rows' lowest heights
     __shared__ alignas(8) uint64_t mbar;
     __shared__ int2 work;
     __shared__ int last_chunk;
     float2* table_buf = air_s[threadIdx.x >> 5];
+    float* rowz_buf = rowz_s[threadIdx.x >> 5];
     const int ntiles = b.ntiles_dev ? *b.ntiles_dev : b.ntiles;
     if (threadIdx.x == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)) : "memory");
@@ -882,11 +1055,13 @@ __global__ void __launch_bounds__(128, 4) k_bp_mixed(MixedBatch b)
             copy_pending = !T.ok;
         }
         if constexpr (!CH) {
-            voxel_mixed<WT, false>(a, m, T, table_buf, R.fp16 != 0, (int64_t)w.y * 128 + threadIdx.x, 0, 0, nullptr);
+            voxel_mixed<WT, false>(a, m, T, table_buf, rowz_buf, R.fp16 != 0, (int64_t)w.y * 128 + threadIdx.x, 0, 0,
+                                   nullptr);
         } else {
             const int p0 = (int)((int64_t)chunk * a.np / K), p1 = (int)((int64_t)(chunk + 1) * a.np / K);
             double2* dst = K == 1 ? a.out : b.chunks[w.x].partial + chunk * ((int64_t)a.nx * a.ny * a.nz);
-            voxel_mixed<WT, true>(a, m, T, table_buf, R.fp16 != 0, (int64_t)tile * 128 + threadIdx.x, p0, p1, dst);
+            voxel_mixed<WT, true>(a, m, T, table_buf, rowz_buf, R.fp16 != 0, (int64_t)tile * 128 + threadIdx.x, p0, p1,
+                                  dst);
             // the work item again from shared memory, so none of it stays live over the pulses
             const volatile int* wv = reinterpret_cast<volatile int*>(&work);
             const int2 w2 = make_int2(wv[0], wv[1]);
@@ -923,6 +1098,7 @@ static MixedCtx mixed_ctx(const DemView& d, int pitch)
     m.idx64 = 1.0 / d.stepx;
     m.idy64 = 1.0 / d.stepy;
     m.start_band = mixed_start_band(d);
+    m.prune = 0;
     return m;
 }
 
@@ -939,7 +1115,8 @@ __global__ void k_refraction_mixed(DemView d, MixedCtx m, const double* __restri
         const float B32[3] = {(float)(B[0] - m.ox), (float)(B[1] - m.oy), (float)B[2]};
         double dA, dB, X[3];
         const VoxelStart vs{height32(m, B32[0], B32[1]), dem_elevation(d, B[0], B[1])};
-        solve_mixed<0, false>(d, m, T, nullptr, A, B, A32, B32, na, nb, true, W, vs, dA, dB, X);
+        int seed = -1;
+        solve_mixed<0, false>(d, m, T, nullptr, nullptr, A, B, A32, B32, na, nb, true, W, vs, seed, dA, dB, X);
         out[3 * k] = X[0];
         out[3 * k + 1] = X[1];
         out[3 * k + 2] = X[2];

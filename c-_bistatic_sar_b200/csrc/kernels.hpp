@@ -95,7 +95,7 @@ struct alignas(64) MixedReq {
     int pitch;            // row pitch (floats), a multiple of 4
     int use_tile;         // tmap valid: stage DEM tiles with TMA
     int fp16;             // samples stored FP16 complex + scale (else complex64)
-    int pad;
+    int exhaustive;       // 1: node scans rank every node (no pruning); the image is the same
     float stepx, stepy, istepx, istepy;
     double ox, oy;        // origin of the FP32 frame (first DEM node)
     double idx64, idy64;  // 1 / spacing

@@ -676,7 +676,7 @@ inline void ensure_mixed_buffers(bsar_ctx* ctx)
 }
 
 // The device record of one mixed-form request.
-inline MixedReq mixed_request(const Scene* s, const BpArgs& a, bool fp16)
+inline MixedReq mixed_request(const Scene* s, const BpArgs& a, bool fp16, int32_t flags)
 {
     MixedReq r;
     std::memset(&r, 0, sizeof r);
@@ -686,6 +686,7 @@ inline MixedReq mixed_request(const Scene* s, const BpArgs& a, bool fp16)
     r.pitch = s->dem.pitch;
     r.use_tile = s->dem.has_tmap ? 1 : 0;
     r.fp16 = fp16 ? 1 : 0;
+    r.exhaustive = (flags & BSAR_BP_EXHAUSTIVE_SCAN) ? 1 : 0;
     r.stepx = (float)s->dem.view.stepx;
     r.stepy = (float)s->dem.view.stepy;
     r.istepx = (float)(1.0 / s->dem.view.stepx);

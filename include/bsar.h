@@ -228,9 +228,15 @@ typedef struct bsar_bp_opts {
     int32_t solver;          /* bsar_solver    */
     int32_t legs;            /* bsar_legs      */
     int32_t precision;       /* bsar_precision */
-    int32_t flags;           /* reserved, 0    */
+    int32_t flags;           /* 0 or BSAR_BP_EXHAUSTIVE_SCAN */
     double search_radius_m;  /* Newton node-scan radius (<= 0: 1.5 m) */
 } bsar_bp_opts;
+
+/* bsar_bp_opts.flags.  BSAR_BP_EXHAUSTIVE_SCAN: the mixed forms rank every node of each
+ * Fermat node-scan window instead of skipping the rows and column groups that a lower
+ * bound proves cannot hold the minimum.  The image is bit-identical either way; the flag
+ * exists to verify that, at the cost of speed.  The FP64 forms always scan every node. */
+enum { BSAR_BP_EXHAUSTIVE_SCAN = 1 };
 
 /* The imager's voxel loop, proc_test_script.cpp:451-767: for every voxel the Fermat
  * solves of all pulses, the delays / phases (:559-577) and the interpolated, phase-

@@ -98,6 +98,42 @@ def test_mixed_matches_fp64(ctx, which, precision, request):
     assert np.argmax(np.abs(img)) == np.argmax(np.abs(ref))
 
 
+@pytest.fixture(scope="module")
+def slab():
+    # medium-scene geometry (256^2 fBm DEM at 0.25 m, eps_r 6) on a 48 x 48 x 3 slab with
+    # 256 consecutive pulses: whole warps of neighbouring voxels, consecutive pulses
+    return _setup(S.scaled(S.config_spec(2), n_pulses=256, n_samples=4096, nx=48, ny=48, nz=3, n_scatterers=5))
+
+
+@pytest.mark.parametrize("precision", ["mixed", "mixed_fp16"])
+@pytest.mark.parametrize("which", ["small", "chunked", "rough", "large", "slab"])
+def test_pruned_node_scan_is_bit_identical(ctx, which, precision, request):
+    """The mixed node scan skips rows and column groups that its lower bound excludes; the
+    image must be bit for bit the one of the scan that ranks every node."""
+    sc = request.getfixturevalue(which)
+    sid = bsar.upload_scene(ctx, sc)
+    try:
+        full = ctx.backproject(sid, sc.gx, sc.gy, sc.gz, solver="newton", legs="per_pulse", precision=precision,
+                               exhaustive=True)
+        pruned = ctx.backproject(sid, sc.gx, sc.gy, sc.gz, solver="newton", legs="per_pulse", precision=precision)
+    finally:
+        ctx.scene_release(sid)
+    assert np.array_equal(pruned, full)
+
+
+def test_unknown_backprojection_flags_are_rejected(ctx, small):
+    sid = bsar.upload_scene(ctx, small)
+    try:
+        keep, g = ctx._grid(small.gx, small.gy, small.gz)
+        out = np.empty((len(small.gx), len(small.gy), len(small.gz)), dtype=np.complex128)
+        o = bsar.native.BpOpts(1, 1, 1, 2, 0.0)          # Newton, per-pulse, mixed, flag bit 1
+        st = ctx.L.bsar_backproject(ctx.h, sid, bsar.native.C.byref(g), bsar.native.C.byref(o),
+                                    bsar.native._p(out.view(np.float64)))
+        assert st == 1
+    finally:
+        ctx.scene_release(sid)
+
+
 @pytest.mark.parametrize("which", ["chunked"])
 def test_mixed_small_grid_pulse_chunks_are_deterministic(ctx, which, request):
     """Grids too small to fill the GPU run each 128-voxel tile's pulses in chunks; the
