@@ -199,10 +199,11 @@ def time_device(ctx, torch, stream, sid, sc, precision, solver, legs, steps, war
     return total_ms, bp_ms, img, ctx.launches - launches0
 
 
-def cpu_reference_rate(sc, seconds: float, threads: int, use_ref: bool = True, z_slices=None):
-    """Reference CPU path (grid search, mean legs) on a bounded voxel sample (uniform over
-    the grid, or over the z-slices `z_slices`).  Returns (voxel-pulses/s for a full image,
-    details incl. the sampled voxels and their values)."""
+def cpu_reference_rate(sc, seconds: float, threads: int, use_ref: bool = True, voxels=None, what=None):
+    """Reference CPU path (grid search, mean legs) on a bounded voxel sample: `voxels`
+    (flat indices in the reference's voxel order) when given, else random voxels of the
+    grid, as many as take about `seconds`.  Returns (voxel-pulses/s for a full image,
+    details incl. the sampled voxels, their values and the upsampled pulses)."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as O
 
@@ -225,36 +226,108 @@ def cpu_reference_rate(sc, seconds: float, threads: int, use_ref: bool = True, z
     else:
         kw["solver"] = "grid"
 
-    def pick(n):
-        if z_slices is None:
-            return rng.choice(nv_total, size=n, replace=False)
-        plane = sp.nx * sp.ny
-        zi = rng.choice(np.asarray(z_slices), size=n)
-        return zi * plane + rng.choice(plane, size=n, replace=True)
-
     last = {}
 
-    def run(n):
-        vox = pick(n)
+    def run(vox):
         t0 = time.perf_counter()
         vals = impl.backproject(dem, sc.tx, sc.rx, rc, sc.gx, sc.gy, sc.gz, sp.n1, sp.n2, 3e8, sc.fs_eff, sc.lam,
                                 voxels=vox, **kw)
         last["vox"], last["vals"] = vox, vals
         return time.perf_counter() - t0
 
-    n0 = max(threads, 1)
-    dt0 = run(n0)
-    n1 = max(n0, int(n0 * seconds / max(dt0, 1e-3)) // n0 * n0)
-    dt1 = run(n1) if n1 > n0 else dt0
+    if voxels is not None:
+        n1 = len(voxels)
+        dt1 = run(np.asarray(voxels, dtype=np.int64))
+        what = what or f"{n1} listed voxels"
+    else:
+        n0 = max(threads, 1)
+        dt0 = run(rng.choice(nv_total, size=n0, replace=False))
+        n1 = max(n0, int(n0 * seconds / max(dt0, 1e-3)) // n0 * n0)
+        dt1 = run(rng.choice(nv_total, size=n1, replace=False)) if n1 > n0 else dt0
+        what = f"{n1} random voxels"
     per_voxel = dt1 / n1
     full_s = t_pc + t_up + per_voxel * nv_total
     rate = nv_total * sp.n_pulses / full_s
     return rate, {"kind": kind, "cores": threads, "sample": (
-        f"{n1} random voxels of the {sp.nx}x{sp.ny}x{sp.nz} grid x {sp.n_pulses} pulses (grid-search Fermat, "
+        f"{what} of the {sp.nx}x{sp.ny}x{sp.nz} grid x {sp.n_pulses} pulses (grid-search Fermat, "
         f"mean legs, as shipped) in {dt1:.1f} s + full pulse compression {t_pc:.1f} s and upsampling "
         f"{t_up:.1f} s; rate = full-image voxel-pulses / (compression + upsampling + per-voxel time x "
-        f"{nv_total} voxels)"), "per_voxel_s": per_voxel, "pc_s": t_pc, "upsample_s": t_up, "voxels": last["vox"],
-        "values": last["vals"]}
+        f"{nv_total} voxels), extrapolated linearly in the voxel count"), "per_voxel_s": per_voxel, "pc_s": t_pc,
+        "upsample_s": t_up, "voxels": last["vox"], "values": last["vals"], "rc": rc}
+
+
+def parity_sample(sp, scat_voxel, seed: int, target: int = 3000):
+    """Seeded parity sample of the imaging grid: a uniform sub-lattice (every s-th voxel on
+    each axis from a random offset, s chosen for about `target` voxels) and the 3 x 3 x 3
+    neighbourhood of every scatterer.  Returns the voxels' grid indices (n, 3) as (ix, iy, iz),
+    the lattice's axis indices, the neighbourhoods' axis ranges and the neighbourhood each
+    voxel belongs to (-1: lattice)."""
+    rng = np.random.default_rng(seed)
+    s = max(1, int(math.ceil((sp.n_voxels / target) ** (1.0 / 3.0))))
+    lat = [np.arange(rng.integers(0, min(s, n)), n, s) for n in (sp.nx, sp.ny, sp.nz)]
+    ii = np.stack(np.meshgrid(*lat, indexing="ij"), axis=-1).reshape(-1, 3)
+    groups = [np.full(len(ii), -1)]
+    hoods = []
+    for k, (x, y, z) in enumerate(np.asarray(scat_voxel)):
+        ax = [np.arange(max(c - 1, 0), min(c + 2, n)) for c, n in ((x, sp.nx), (y, sp.ny), (z, sp.nz))]
+        hoods.append(ax)
+        h = np.stack(np.meshgrid(*ax, indexing="ij"), axis=-1).reshape(-1, 3)
+        ii = np.concatenate([ii, h])
+        groups.append(np.full(len(h), k))
+    return ii, lat, hoods, np.concatenate(groups)
+
+
+def flat_voxels(sp, ii):
+    """Grid indices (ix, iy, iz) -> the reference's flat voxel order (z -> x -> y)."""
+    return (ii[:, 2] * sp.nx + ii[:, 0]) * sp.ny + ii[:, 1]
+
+
+def sample_stats(x, ref, groups):
+    """Errors of sample values x against ref: rel-L2, max phase error over the voxels at or
+    above 1e-3 of the largest magnitude, the sample's argmax, and per scatterer whether the
+    argmax of its 3 x 3 x 3 neighbourhood is the same voxel."""
+    m = np.abs(ref) >= 1e-3 * np.abs(ref).max()
+    hood = [np.flatnonzero(groups == k) for k in range(int(groups.max()) + 1)]
+    same = sum(int(np.argmax(np.abs(x[h])) == np.argmax(np.abs(ref[h]))) for h in hood if len(h))
+    return {"rel_l2": float(np.linalg.norm(x - ref) / np.linalg.norm(ref)),
+            "max_abs": float(np.abs(x - ref).max()),
+            "max_phase_err_rad": float(np.abs(np.angle(x[m] * np.conj(ref[m]))).max()),
+            "argmax_match": bool(np.argmax(np.abs(x)) == np.argmax(np.abs(ref))),
+            "scatterer_argmax_match": f"{same}/{len(hood)}"}
+
+
+def parity_block(ctx, sid, sc, ii, lat, hoods, groups, det, full_images, W):
+    """Every form on the parity sample against the CPU: the GPU reference algorithm (grid
+    search, mean legs, FP64) against the reference's own compiled code on the same voxels;
+    the GPU FP64 Newton, mixed and mixed-FP16 images (the full-grid images of this run,
+    read at the sample voxels) against the oracle's FP64 Newton on those voxels."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+
+    sp = sc.spec
+    # GPU reference algorithm on the sample: the lattice as one grid, each neighbourhood as
+    # one 3 x 3 x 3 grid (a voxel's FP64 value does not depend on the grid around it)
+    parts = [ctx.backproject(sid, sc.gx[lat[0]], sc.gy[lat[1]], sc.gz[lat[2]], solver="grid", legs="mean",
+                             precision="fp64").reshape(-1)]
+    for ax in hoods:
+        parts.append(ctx.backproject(sid, sc.gx[ax[0]], sc.gy[ax[1]], sc.gz[ax[2]], solver="grid", legs="mean",
+                                     precision="fp64").reshape(-1))
+    gpu_grid = np.concatenate(parts)
+    t = time.perf_counter()
+    orc = O.Oracle().backproject(O.Dem(sc.x_vec, sc.y_vec, sc.z), sc.tx, sc.rx, det["rc"], sc.gx, sc.gy, sc.gz, sp.n1,
+                                 sp.n2, 3e8, sc.fs_eff, sc.lam, legs="per_pulse", solver="newton",
+                                 voxels=flat_voxels(sp, ii), search_nodes=W)
+    t_orc = time.perf_counter() - t
+    at = (ii[:, 0], ii[:, 1], ii[:, 2])
+    return {"voxels": int(len(ii)),
+            "sample": (f"uniform sub-lattice {len(lat[0])}x{len(lat[1])}x{len(lat[2])} (seeded offsets) + 3x3x3 around "
+                       f"each of {len(hoods)} scatterers"),
+            "fp64_grid_mean_vs_reference": sample_stats(gpu_grid, det["values"], groups),
+            "fp64_newton_vs_oracle": sample_stats(full_images["fp64_newton"][at], orc, groups),
+            "mixed_vs_oracle": sample_stats(full_images["mixed"][at], orc, groups),
+            "mixed_fp16_vs_oracle": sample_stats(full_images["mixed_fp16"][at], orc, groups),
+            "oracle_newton_cpu_s": t_orc,
+            "bars": "FP64 forms rel-L2 <= 1e-9; mixed forms rel-L2 <= 1e-3, phase <= 0.01 rad; same argmax"}
 
 
 def serve_leg(ctx, torch, n_requests: int, burst: int, fp64_sample: int, load: float = 0.8, tiles: int = 0):
@@ -508,6 +581,7 @@ def main():
     # ---------------- comparator forms + accuracy ----------------------------------
     forms = {}
     acc = {}
+    full_images = None
     if not args.no_forms:
         fs = max(1, min(2, args.steps))
         t64, bp64, img64, _ = time_device(ctx, torch, stream, sid, sc, "fp64", "newton", "per_pulse", fs, 1)
@@ -537,6 +611,7 @@ def main():
 
         acc = {"mixed_vs_fp64": stats(a), "mixed_fp16_vs_fp64": stats(c16),
                "e2e_image_equals_device_image": bool(np.array_equal(img_host, a))}
+        full_images = {"fp64_newton": b, "mixed": a, "mixed_fp16": c16}
         # Fermat crossing points of the mixed solver against FP64 on random (pulse, voxel) pairs
         rng = np.random.default_rng(0x5A4B0D)
         pi = rng.integers(0, sp.n_pulses, 1 << 16)
@@ -598,18 +673,16 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        zs = list(range(0, sp.nz, 20)) if forms else None
-        rate, det = cpu_reference_rate(sc, args.ref_seconds, threads, z_slices=zs)
+        # the parity sample: the reference's own code runs on it (timed: the CPU baseline)
+        # and every GPU form is compared with it or with the oracle's FP64 Newton on it
+        ii, lat, hoods, groups = parity_sample(sp, sc.scat_voxel, 0x5A4B0002 + args.config)
+        what = (f"{len(ii)} parity-sample voxels ({int((groups < 0).sum())} on a uniform sub-lattice "
+                f"+ the 3x3x3 neighbourhoods of {len(hoods)} scatterers)")
+        rate, det = cpu_reference_rate(sc, args.ref_seconds, threads, voxels=flat_voxels(sp, ii), what=what)
         cpu = {"value": rate, "unit": UNIT, "cores": det["cores"], "kind": det["kind"], "sample": det["sample"]}
-        if zs is not None:
-            v = det["voxels"]
-            plane = sp.nx * sp.ny
-            zi, xi, yi = v // plane, (v % plane) // sp.ny, v % sp.ny
-            g = img_grid[xi, yi, zi // 20]
-            ref = det["values"]
-            cpu["check_vs_gpu_fp64_grid"] = {
-                "voxels": int(len(v)), "rel_l2": float(np.linalg.norm(g - ref) / np.linalg.norm(ref)),
-                "max_abs": float(np.abs(g - ref).max())}
+        if full_images is not None:
+            acc["vs_oracle_sample"] = parity_block(ctx, sid, sc, ii, lat, hoods, groups, det, full_images, W)
+        del det
         shipped = min(12, threads)
         if shipped != threads:
             r12, d12 = cpu_reference_rate(sc, args.ref_seconds, shipped)

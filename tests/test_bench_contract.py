@@ -39,3 +39,35 @@ def test_reference_arm_line():
 def test_reference_arm_other_ranks_exit_quietly():
     r = _run({"RANK": "1", "WORLD_SIZE": "2"})
     assert r.returncode == 0 and r.stdout.strip() == ""
+
+
+def test_parity_sample_covers_the_medium_scene():
+    """The medium scene's parity sample: at least 4096 voxels, a uniform sub-lattice plus
+    the full 3 x 3 x 3 neighbourhood of each of the 50 scatterers, mapped to the
+    reference's flat voxel order (z -> x -> y, y fastest)."""
+    import numpy as np
+    sys.path.insert(0, str(ROOT))
+    sys.path.insert(0, str(ROOT / "c-_bistatic_sar_b200"))
+    import bench
+    from bsar import scene as S
+
+    sp = S.config_spec(2)
+    _, rs, _, _ = S._streams(sp.seed)
+    gx, gy, gz = S.grid_axes(sp)
+    _, _, sv = S.make_scatterers(sp, rs, gx, gy, gz)
+    ii, lat, hoods, groups = bench.parity_sample(sp, sv, 0x5A4B0004)
+    assert len(ii) >= 4096 and len(hoods) == 50
+    for k, (x, y, z) in enumerate(sv):
+        h = ii[groups == k]
+        assert len(h) == 27 and (np.abs(h - [x, y, z]).max(axis=1) <= 1).all()
+    lat_ii = ii[groups < 0]
+    assert len(lat_ii) == len(lat[0]) * len(lat[1]) * len(lat[2])
+    v = bench.flat_voxels(sp, ii)
+    assert ((v % sp.ny == ii[:, 1]) & ((v // sp.ny) % sp.nx == ii[:, 0]) & (v // (sp.nx * sp.ny) == ii[:, 2])).all()
+    # statistics: identical values match exactly; a perturbed copy is measured
+    rng = np.random.default_rng(0)
+    ref = rng.normal(size=len(ii)) + 1j * rng.normal(size=len(ii))
+    st = bench.sample_stats(ref, ref, groups)
+    assert st["rel_l2"] == 0.0 and st["argmax_match"] and st["scatterer_argmax_match"] == "50/50"
+    st = bench.sample_stats(ref * np.exp(0.002j), ref, groups)
+    assert abs(st["max_phase_err_rad"] - 0.002) < 1e-9
