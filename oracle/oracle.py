@@ -225,6 +225,9 @@ class Reference:
         L.ref_export_complex_matrix.argtypes = [C.c_char_p, _i64, _i64, _d]
         L.ref_export_3d.argtypes = [C.c_char_p, _i64, _i64, _i64, _d, _d, _d, _d]
         L.ref_load_dem.argtypes = [C.c_char_p, C.POINTER(_i64), C.POINTER(_i64), _d, _d, _d]
+        L.ref_process_raw_data.argtypes = ([_i64, _d, _d, _d, _d] + [C.c_double] * 7 +
+                                           [_i32, C.c_double, C.c_double, _d, _d, _d, _d, _i64])
+        L.ref_process_raw_data.restype = _i64
         L.ref_backproject.argtypes = dem5 + [_d, _d, _i64, _d, _i64, _d, _i64, _d, _i64, _d, _i64,
                                              C.c_double, C.c_double, C.c_double, C.c_double,
                                              C.c_double, _i32, C.POINTER(_i64), _i64, _i32, _d]
@@ -286,6 +289,22 @@ class Reference:
         out = np.empty(n, dtype=np.complex128)
         got = self.L.ref_create_chirp(f0, f1, T, fs, _ptr(out.view(np.float64)), n)
         return out[:got]
+
+    def process_raw_data(self, tx, rx, P, ranges, f0, f1, T, fs, lamb, rcs, c, M, n1, n2):
+        """processRawData on given ranges (4 x np: r1Tx, r2Tx, r1Rx, r2Rx); returns the
+        pulse-major (np x M) aux, raw and root matrices and the chirp."""
+        tx = _f64(tx, (-1, 3))
+        rx = _f64(rx, (-1, 3))
+        P = _f64(P, (3,))
+        ranges = _f64(ranges, (4, -1))
+        n = len(tx)
+        aux, raw, root = (np.empty((n, M), dtype=np.complex128) for _ in range(3))
+        cap = int(T * fs) + 2
+        chirp = np.empty(cap, dtype=np.complex128)
+        got = self.L.ref_process_raw_data(n, _ptr(tx), _ptr(rx), _ptr(P), _ptr(ranges), f0, f1, T, fs, lamb, rcs, c,
+                                          M, n1, n2, _ptr(aux.view(np.float64)), _ptr(raw.view(np.float64)),
+                                          _ptr(root.view(np.float64)), _ptr(chirp.view(np.float64)), cap)
+        return aux, raw, root, chirp[:got]
 
     def backproject(self, dem: Dem, tx, rx, rc, gx, gy, gz, n1, n2, c, fs_eff, lam,
                     legs="mean", voxels=None, nthreads=0):

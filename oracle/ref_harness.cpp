@@ -340,6 +340,66 @@ void ref_export_3d(const char* path, int64_t nx, int64_t ny, int64_t nz, const d
     export3DComplexMatrix(path, o, nx, ny, nz, ax, ay, az);
 }
 
+// The simulator's processRawData (src/raw_data_processing.cpp:292-452) on given per-pulse
+// ranges (r1Tx, r2Tx, r1Rx, r2Rx, each np long): one target of cross section rcs, an
+// M-sample pulse (System::IndiceMaximo), the chirp f0 -> f1 over T at fs, wavelength lamb.
+// Outputs are pulse-major (np x M complex): aux (the placed deltas), raw (after the
+// convolution with the fftshifted chirp) and root (after pulse compression); chirp gets
+// createCHIRP's samples (returns their count).
+int64_t ref_process_raw_data(int64_t np, const double* tx, const double* rx, const double* P, const double* ranges,
+                             double f0, double f1, double T, double fs, double lamb, double rcs, double c, int32_t M,
+                             double n1, double n2, double* aux, double* raw, double* root, double* chirp,
+                             int64_t chirp_cap)
+{
+    TrajectoryMatrix traj;
+    traj.Tx = make_points(tx, np);
+    traj.Rx = make_points(rx, np);
+    traj.P = {P[0], P[1], P[2]};
+    RangeData r;
+    r.r1Tx.assign(ranges, ranges + np);
+    r.r2Tx.assign(ranges + np, ranges + 2 * np);
+    r.r1Rx.assign(ranges + 2 * np, ranges + 3 * np);
+    r.r2Rx.assign(ranges + 3 * np, ranges + 4 * np);
+    RadarTx rtx{};
+    rtx.FreqMenor = f0;
+    rtx.FreqMaior = f1;
+    rtx.DuracaoPulso = T;
+    rtx.fs = fs;
+    rtx.lamb = lamb;
+    RadarRx rrx{};
+    rrx.fs = fs;
+    Target tg{};
+    tg.pos[0] = P[0];
+    tg.pos[1] = P[1];
+    tg.pos[2] = P[2];
+    tg.rcs = rcs;
+    System sys{};
+    sys.VelocidadeLuz = c;
+    sys.IndiceMaximo = M;
+    sys.NumeroPulsos = (int)np;
+    Environment env{n1, n2};
+    RawDataResult res;
+    {
+        QuietStdout q(true);
+        res = processRawData(traj, r, rtx, rrx, tg, sys, env);
+    }
+    for (int64_t i = 0; i < np; i++)
+        for (int32_t b = 0; b < M; b++) {
+            const int64_t o = 2 * (i * M + b);
+            aux[o] = res.auxData[b][i].real();
+            aux[o + 1] = res.auxData[b][i].imag();
+            raw[o] = res.rawData[b][i].real();
+            raw[o + 1] = res.rawData[b][i].imag();
+            root[o] = res.rootData[b][i].real();
+            root[o + 1] = res.rootData[b][i].imag();
+        }
+    for (int64_t k = 0; k < (int64_t)res.chirp.size() && k < chirp_cap; k++) {
+        chirp[2 * k] = res.chirp[k].real();
+        chirp[2 * k + 1] = res.chirp[k].imag();
+    }
+    return (int64_t)res.chirp.size();
+}
+
 // loadDEM (src/load_dem_simple.cpp:9-224): sizes first (z == NULL), then the arrays
 // (z[j*nx + i] = Z_DEM[j][i]; rows shorter than nx read as 0).
 void ref_load_dem(const char* path, int64_t* nx, int64_t* ny, double* xv, double* yv, double* z)

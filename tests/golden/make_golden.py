@@ -10,6 +10,9 @@ from it by oracle/Makefile).  Writes:
                          FFTProcessor::fft / ifft / fftCorrelation / fftConvolution,
                          createCHIRP, and the inline back-projection of
                          proc_test_script.cpp (mean and per-pulse legs)
+  raw_data_vectors.npz   processRawData of the simulator on one target and 6 pulses:
+                         the placed deltas (auxData), raw echoes (rawData) and compressed
+                         pulses (rootData), with the ranges and radar it ran on
   cfg1_image.npz         the full 41 x 41 x 21 image of the config-1 scene (256 pulses)
                          from the reference's back-projection (grid search, mean legs),
                          with a fingerprint of the generated inputs
@@ -85,6 +88,40 @@ def small_vectors(ref: O.Reference):
                 bp_per=bp_per, bp_scalars=np.array([bp_args[k] for k in ("n1", "n2", "c", "fs_eff", "lam")]))
 
 
+def raw_vectors(ref: O.Reference, orc: O.Oracle):
+    """The simulator's processRawData (src/raw_data_processing.cpp:292-452) for one target
+    over 6 pulses, on ranges from the FP64 Newton crossings of the oracle (the solver the
+    GPU echo synthesis runs, bit for bit): the placed deltas, the raw echoes and the
+    compressed pulses, 1024 samples each."""
+    rng = np.random.default_rng(20241)
+    n = 32
+    xv = 20.0 + (np.arange(n) - (n - 1) / 2.0) * 0.25
+    yv = (np.arange(n) - (n - 1) / 2.0) * 0.25
+    z = rng.normal(0.0, 0.04, size=(n, n))
+    dem = O.Dem(xv, yv, z)
+    s = np.arange(6) / 5.0
+    tx = np.stack([15 * (1 - s) * np.cos(2 * np.pi * s), 15 * (1 - s) * np.sin(2 * np.pi * s), np.full(6, 30.0)], 1)
+    rx = tx + np.array([5.0, 0.0, 0.0])
+    P = np.array([20.05, -0.12, -5.03])
+    n1, n2, c, fc, fs, f0, f1, T, M, rcs = 1.0, 2.0, 3e8, 1e9, 1.2e9, -250e6, 250e6, 1e-7, 1024, 0.8
+    W = S.search_nodes_for(xv, yv)
+    Pn = np.repeat(P[None], len(tx), 0)
+    a = orc.refraction_points(dem, tx, Pn, n1, n2, solver="newton", search_nodes=W)
+    b = orc.refraction_points(dem, Pn, rx, n2, n1, solver="newton", search_nodes=W)
+
+    def dist(u, w):
+        # the synthesis kernel's distance: sqrt(x*x + y*y + z*z) of u - w, in that order
+        return np.array([float(np.sqrt((p[0] - q[0]) * (p[0] - q[0]) + (p[1] - q[1]) * (p[1] - q[1])
+                                       + (p[2] - q[2]) * (p[2] - q[2]))) for p, q in zip(u, w)])
+
+    ranges = np.stack([dist(tx, a), dist(Pn, a), dist(rx, b), dist(Pn, b)])    # r1Tx, r2Tx, r1Rx, r2Rx
+    assert np.all(np.isfinite(ranges)) and np.all(ranges > 0)
+    aux, raw, root, chirp = ref.process_raw_data(tx, rx, P, ranges, f0, f1, T, fs, c / fc, rcs, c, M, n1, n2)
+    return dict(raw_dem_x=xv, raw_dem_y=yv, raw_dem_z=z, raw_tx=tx, raw_rx=rx, raw_P=P, raw_ranges=ranges,
+                raw_scalars=np.array([n1, n2, c, fc, fs, f0, f1, T, M, rcs]), raw_aux=aux, raw_raw=raw,
+                raw_root=root, raw_chirp=chirp)
+
+
 def cfg1_image(ref: O.Reference):
     spec = S.config_spec(1)
     sc = S.make_scene(spec)
@@ -106,6 +143,8 @@ def main():
     ref = O.Reference()
     np.savez_compressed(HERE / "reference_vectors.npz", **small_vectors(ref))
     print("wrote", HERE / "reference_vectors.npz")
+    np.savez_compressed(HERE / "raw_data_vectors.npz", **raw_vectors(ref, O.Oracle()))
+    print("wrote", HERE / "raw_data_vectors.npz")
     if not args.skip_image:
         np.savez_compressed(HERE / "cfg1_image.npz", **cfg1_image(ref))
         print("wrote", HERE / "cfg1_image.npz")
