@@ -67,6 +67,7 @@ struct MixedCtx {
     double idx64, idy64;            // 1 / spacing, FP64
     float start_band;               // node units: FP32 starts this close to a cell boundary go FP64
     int prune;                      // node scans may skip what the lower bound excludes
+    float zmin;                     // lowest FP32 height of the DEM
 };
 
 // Start heights under a voxel (the lower endpoint of both of its paths when the ground
@@ -309,57 +310,34 @@ template <int WT> struct TableRows { static constexpr int v = WT > 0 ? 2 * WT + 
 
 struct AirTable {
     float2* t;
-    float* rowz;        // lowest height of each table row (over the table's columns)
     int i0, j0;
-    float zmin;         // lowest height of the whole table
     bool ok;
 };
 
-// Float <-> unsigned key with the same order (for the warp min reduction of heights).
-__device__ __forceinline__ unsigned order_key(float f)
-{
-    const unsigned u = __float_as_uint(f);
-    return (u >> 31) ? ~u : (u | 0x80000000u);
-}
-__device__ __forceinline__ float order_key_float(unsigned k)
-{
-    return __uint_as_float((k >> 31) ? (k & 0x7fffffffu) : ~k);
-}
-
 template <int TBI>
-__device__ __forceinline__ AirTable build_air_table(const MixedCtx& m, const Tile& T, float2* buf, float* rowz, int is,
-                                                    int js, int W, float ex, float ey, float ez, float re)
+__device__ __forceinline__ AirTable build_air_table(const MixedCtx& m, const Tile& T, float2* buf, int is, int js, int W,
+                                                    float ex, float ey, float ez, float re)
 {
     const unsigned full = 0xffffffffu;
     int i0 = max(__reduce_min_sync(full, is) - W, 0), i1 = min(__reduce_max_sync(full, is) + W, m.nx - 1);
     int j0 = max(__reduce_min_sync(full, js) - W, 0), j1 = min(__reduce_max_sync(full, js) + W, m.ny - 1);
-    AirTable A{buf, rowz, i0, j0, INFINITY, false};
+    AirTable A{buf, i0, j0, false};
     __syncwarp();                       // readers of the previous table are done
     if (i1 - i0 + 1 > TBI || j1 - j0 + 1 > TBJ) return A;
     const int lane = threadIdx.x & 31;
     const int j = j0 + lane;
-    const bool col = j <= j1;
     const bool in_tile = T.ok && i0 >= T.i0 && i1 < T.i0 + TI && j0 >= T.j0 && j1 < T.j0 + TJ;
-    float dy = (float)j * m.stepy - ey;
-    float sy = dy * dy;
-    unsigned kmin = 0xffffffffu;
-    // every lane walks the rows (the row minimum is a warp reduction); lanes right of the
-    // union's last column only take part in it
-    for (int i = i0; i <= i1; i++) {
-        unsigned key = 0xffffffffu;
-        if (col) {
+    if (j <= j1) {
+        float dy = (float)j * m.stepy - ey;
+        float sy = dy * dy;
+        for (int i = i0; i <= i1; i++) {
             float z = in_tile ? T.s[(j - T.j0) * TI + (i - T.i0)] : zf(m, i, j);
             float dx = (float)i * m.stepx - ex, dz = z - ez;
             float q = fmaf(dz, dz, fmaf(dx, dx, sy));
             buf[(i - i0) * TBJ + lane] = make_float2(z, re * (q * rsqrtf(q)));
-            key = order_key(z);
         }
-        const unsigned rk = __reduce_min_sync(full, key);
-        kmin = min(kmin, rk);
-        if (lane == 0) rowz[i - i0] = order_key_float(rk);
     }
     __syncwarp();
-    A.zmin = order_key_float(kmin);
     A.ok = true;
     return A;
 }
@@ -367,10 +345,15 @@ __device__ __forceinline__ AirTable build_air_table(const MixedCtx& m, const Til
 // Full (2W+1)^2 window inside the DEM and the warp table: height and E leg from the
 // table (one 8-byte load per node), the G leg per node, columns unrolled with
 // compile-time offsets.  The best node's row is updated once per row.
+// Out of line: it runs for the exhaustive flag and for warps whose lanes do not all have
+// full windows, so its body stays out of the pulse loop's instruction stream.
 template <int W>
-__device__ __forceinline__ void scan_table(const MixedCtx& m, const AirTable& AT, int is, int js, float gx, float gy,
-                                           float gz, float& v1, float& v2, int& bi, int& bj)
+__device__ __noinline__ Rank scan_table(const MixedCtx m, const float2* tab, int ti0, int tj0, int is, int js, float gx,
+                                        float gy, float gz, Rank rk)
 {
+    float v1 = rk.v1, v2 = rk.v2;
+    int bi = rk.bi, bj = rk.bj;
+    const AirTable AT{const_cast<float2*>(tab), ti0, tj0, true};
     constexpr int NJ = 2 * W + 1;
     float syg[NJ];
 #pragma unroll
@@ -401,6 +384,7 @@ __device__ __forceinline__ void scan_table(const MixedCtx& m, const AirTable& AT
         bi = (v1 < v1_row) ? i : bi;
     }
     bj = js - W + bc;
+    return Rank{v1, v2, bi, bj};
 }
 
 // Columns of a window row in groups of four for the pruned scan; a trailing single column
@@ -461,8 +445,9 @@ __device__ __forceinline__ void scan_pruned(const MixedCtx& m, const AirTable& A
     const float yv_t = -ay / sy2;                       // vertex of the parabola: Y = t * yv_t
     const float ay2 = 2.0f * ay;
     const float yfirst = (float)(js - W) * m.stepy - gy;
-    // height monotonicity over the window (else nothing is pruned)
-    const float Zt = AT.zmin - gz;
+    // height monotonicity over the window, from the DEM's lowest height (else nothing is
+    // pruned)
+    const float Zt = m.zmin - gz;
     const float hx = fabsf(x0 - gx) + (float)W * m.stepx, hy = fabsf(y0 - gy) + (float)W * m.stepy;
     const bool bound_ok = sy2 > 1e-3f &&           // |a| = re: the bound needs the E leg's index below the G leg's
                           (az >= 0.0f || (Zt > 0.0f && az * az * (hx * hx + hy * hy + Zt * Zt) <= Zt * Zt));
@@ -478,7 +463,7 @@ __device__ __forceinline__ void scan_pruned(const MixedCtx& m, const AirTable& A
             thr_seed = fmaf(q, rsqrtf(q), e.y);
         }
     }
-    const float never = bound_ok ? 0.0f : INFINITY;     // +inf: keep every row
+    const float never = bound_ok ? 0.0f : INFINITY;     // +inf: keep every node
     int bc = bj - (js - W);
 #pragma unroll 1
     for (int k = 0; k < NJ; k++) {
@@ -488,28 +473,34 @@ __device__ __forceinline__ void scan_pruned(const MixedCtx& m, const AirTable& A
         const float dx = (float)i * m.stepx - gx;
         const float sxg = dx * dx;
         const float2* row = row0 + r * TBJ;
-        const float v1_row = v1;
         float T = fminf(thr_seed, v1) + tie + never;
         T = T + fmaf(4e-6f, fabsf(T), 2e-4f);
         const float R = T - K - ax * dx;
+        float2 e[NJ];
+#pragma unroll
+        for (int c = 0; c < NJ; c++) e[c] = row[c];
+        float zg[CG::N];
+#pragma unroll
+        for (int g = 0; g < CG::N; g++) {
+            zg[g] = e[CG::first(g)].x;
+#pragma unroll
+            for (int c = CG::first(g) + 1; c <= CG::last(g); c++) zg[g] = fminf(zg[g], e[c].x);
+        }
+        // the whole row (Y free) against its lowest height
         {
-            const float zl = AT.rowz[i - AT.i0] - gz;
+            float zr = zg[0];
+#pragma unroll
+            for (int g = 1; g < CG::N; g++) zr = fminf(zr, zg[g]);
+            const float zl = zr - gz;
             const float t = R - az * zl;
             const bool skip = t < 0.0f || t * t < sy2 * fmaf(zl, zl, sxg);
             if (!__any_sync(full, !skip)) continue;
         }
+        const float v1_row = v1;
 #pragma unroll
         for (int g = 0; g < CG::N; g++) {
             const int c0 = CG::first(g), c1 = CG::last(g);
-            float2 e[5];
-            float zc = INFINITY;
-#pragma unroll
-            for (int c = 0; c < 5; c++)
-                if (c0 + c <= c1) {
-                    e[c] = row[c0 + c];
-                    zc = fminf(zc, e[c].x);
-                }
-            const float zl = zc - gz;
+            const float zl = zg[g] - gz;
             const float t = R - az * zl;
             const float ylo = fmaf((float)c0, m.stepy, yfirst), yhi = fmaf((float)c1, m.stepy, yfirst);
             const float yc = fminf(fmaxf(t * yv_t, ylo), yhi);
@@ -517,16 +508,15 @@ __device__ __forceinline__ void scan_pruned(const MixedCtx& m, const AirTable& A
             const bool skip = t < 0.0f || q > 0.0f;
             if (!__any_sync(full, !skip)) continue;
 #pragma unroll
-            for (int c = 0; c < 5; c++)
-                if (c0 + c <= c1) {
-                    const float dz = e[c].x - gz;
-                    const float qq = fmaf(dz, dz, sxg + syg[c0 + c]);
-                    const float L = fmaf(qq, rsqrtf(qq), e[c].y);
-                    v2 = fminf(v2, fmaxf(v1, L));
-                    const bool p = L < v1;
-                    v1 = p ? L : v1;
-                    bc = p ? c0 + c : bc;
-                }
+            for (int c = c0; c <= c1; c++) {
+                const float dz = e[c].x - gz;
+                const float qq = fmaf(dz, dz, sxg + syg[c]);
+                const float L = fmaf(qq, rsqrtf(qq), e[c].y);
+                v2 = fminf(v2, fmaxf(v1, L));
+                const bool p = L < v1;
+                v1 = p ? L : v1;
+                bc = p ? c : bc;
+            }
         }
         bi = (v1 < v1_row) ? i : bi;
     }
@@ -550,7 +540,11 @@ __device__ __forceinline__ void node_scan(const MixedCtx& m, const Tile& T, cons
             return;
         }
         if (full_window) {
-            scan_table<W>(m, AT, is, js, G[0], G[1], G[2], v1, v2, bi, bj);
+            const Rank r = scan_table<W>(m, AT.t, AT.i0, AT.j0, is, js, G[0], G[1], G[2], Rank{v1, v2, bi, bj});
+            v1 = r.v1;
+            v2 = r.v2;
+            bi = r.bi;
+            bj = r.bj;
             return;
         }
     }
@@ -679,7 +673,7 @@ __device__ __noinline__ int2 start_node64(const DemView d, double Ax, double Ay,
 // ((i << 16) | j, or -1), which only speeds up the pruned scan; out, the node chosen now.
 template <int WT, bool TABLE>
 __device__ __forceinline__ double solve_mixed(const DemView& d, const MixedCtx& m, const Tile& T, float2* table_buf,
-                                              float* rowz_buf, const double A[3], const double B[3],
+                                              const double A[3], const double B[3],
                                               const float A32[3], const float B32[3], float na, float nb,
                                               bool g_is_b, int W, const VoxelStart& vs, int& seed, double& dA,
                                               double& dB, double* X = nullptr)
@@ -726,9 +720,9 @@ __device__ __forceinline__ double solve_mixed(const DemView& d, const MixedCtx& 
     const float* G = g_is_b ? B32 : A32;
     const float ng = g_is_b ? nb : na;
     const float re = (g_is_b ? na : nb) / ng;
-    AirTable AT{table_buf, rowz_buf, 0, 0, INFINITY, false};
+    AirTable AT{table_buf, 0, 0, false};
     if constexpr (TABLE && WT > 0)
-        AT = build_air_table<TableRows<WT>::v>(m, T, table_buf, rowz_buf, is, js, W, E[0], E[1], E[2], re);
+        AT = build_air_table<TableRows<WT>::v>(m, T, table_buf, is, js, W, E[0], E[1], E[2], re);
     float v1 = INFINITY, v2 = INFINITY;
     int bi = is, bj = js;
     const float tie = kTieM / ng;
@@ -867,6 +861,7 @@ __device__ __forceinline__ MixedCtx req_ctx(const MixedReq& r)
     m.idy64 = r.idy64;
     m.start_band = r.start_band;
     m.prune = !r.exhaustive;
+    m.zmin = r.zmin;
     return m;
 }
 
@@ -875,7 +870,7 @@ __device__ __forceinline__ MixedCtx req_ctx(const MixedReq& r)
 // The sum goes to dst at the voxel's image index.
 template <int WT, bool CH>
 __device__ __forceinline__ void voxel_mixed(const BpArgs& a, const MixedCtx& m, const Tile& T, float2* table_buf,
-                                            float* rowz_buf, bool fp16, int64_t kk, int p0, int p1,
+                                            bool fp16, int64_t kk, int p0, int p1,
                                             double2* __restrict__ dst)
 {
     const int np = CH ? p1 : a.np;
@@ -910,7 +905,7 @@ __device__ __forceinline__ void voxel_mixed(const BpArgs& a, const MixedCtx& m, 
             const float B32[3] = {leg ? R32[0] : P32[0], leg ? R32[1] : P32[1], leg ? R32[2] : P32[2]};
             double dA, dB;
             int seed = leg ? seed1 : seed0;
-            L += solve_mixed<WT, true>(a.dem, m, T, table_buf, rowz_buf, A, B, A32, B32, leg ? n2f : n1f,
+            L += solve_mixed<WT, true>(a.dem, m, T, table_buf, A, B, A32, B32, leg ? n2f : n1f,
                                        leg ? n1f : n2f, leg == 0, a.W, vs, seed, dA, dB);
             seed1 = leg ? seed : seed1;
             seed0 = leg ? seed0 : seed;
@@ -1009,12 +1004,10 @@ __global__ void __launch_bounds__(128, 4) k_bp_mixed(MixedBatch b)
 {
     __shared__ alignas(128) float tile_s[TI * TJ];
     __shared__ alignas(16) float2 air_s[4][TableRows<WT>::v * TBJ];   // one (z, E-leg) table per warp
-    __shared__ float rowz_s[4][TableRows<WT>::v];                        // its rows' lowest heights
     __shared__ alignas(8) uint64_t mbar;
     __shared__ int2 work;
     __shared__ int last_chunk;
     float2* table_buf = air_s[threadIdx.x >> 5];
-    float* rowz_buf = rowz_s[threadIdx.x >> 5];
     const int ntiles = b.ntiles_dev ? *b.ntiles_dev : b.ntiles;
     if (threadIdx.x == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)) : "memory");
@@ -1055,12 +1048,12 @@ __global__ void __launch_bounds__(128, 4) k_bp_mixed(MixedBatch b)
             copy_pending = !T.ok;
         }
         if constexpr (!CH) {
-            voxel_mixed<WT, false>(a, m, T, table_buf, rowz_buf, R.fp16 != 0, (int64_t)w.y * 128 + threadIdx.x, 0, 0,
+            voxel_mixed<WT, false>(a, m, T, table_buf, R.fp16 != 0, (int64_t)w.y * 128 + threadIdx.x, 0, 0,
                                    nullptr);
         } else {
             const int p0 = (int)((int64_t)chunk * a.np / K), p1 = (int)((int64_t)(chunk + 1) * a.np / K);
             double2* dst = K == 1 ? a.out : b.chunks[w.x].partial + chunk * ((int64_t)a.nx * a.ny * a.nz);
-            voxel_mixed<WT, true>(a, m, T, table_buf, rowz_buf, R.fp16 != 0, (int64_t)tile * 128 + threadIdx.x, p0, p1,
+            voxel_mixed<WT, true>(a, m, T, table_buf, R.fp16 != 0, (int64_t)tile * 128 + threadIdx.x, p0, p1,
                                   dst);
             // the work item again from shared memory, so none of it stays live over the pulses
             const volatile int* wv = reinterpret_cast<volatile int*>(&work);
@@ -1099,6 +1092,7 @@ static MixedCtx mixed_ctx(const DemView& d, int pitch)
     m.idy64 = 1.0 / d.stepy;
     m.start_band = mixed_start_band(d);
     m.prune = 0;
+    m.zmin = -INFINITY;
     return m;
 }
 
@@ -1116,7 +1110,7 @@ __global__ void k_refraction_mixed(DemView d, MixedCtx m, const double* __restri
         double dA, dB, X[3];
         const VoxelStart vs{height32(m, B32[0], B32[1]), dem_elevation(d, B[0], B[1])};
         int seed = -1;
-        solve_mixed<0, false>(d, m, T, nullptr, nullptr, A, B, A32, B32, na, nb, true, W, vs, seed, dA, dB, X);
+        solve_mixed<0, false>(d, m, T, nullptr, A, B, A32, B32, na, nb, true, W, vs, seed, dA, dB, X);
         out[3 * k] = X[0];
         out[3 * k + 1] = X[1];
         out[3 * k + 2] = X[2];

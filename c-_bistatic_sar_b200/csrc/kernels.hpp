@@ -101,7 +101,7 @@ struct alignas(64) MixedReq {
     double idx64, idy64;  // 1 / spacing
     float off_x, off_y;   // mean crossing offset from the voxel, metres (tile centring)
     float start_band;     // node units: FP32 flat starts this close to a cell boundary are redone in FP64
-    float pad2;
+    float zmin;           // lowest FP32 height of the DEM (bounds of the pruned node scan)
 };
 
 // Pulse chunks of a request (kept beside MixedReq, read only by the chunked kernel).

@@ -221,6 +221,7 @@ struct DemDev {
     std::unique_ptr<DevBuf> xv, yv, z, z32;
     DemView view{};
     int pitch = 0;                                  // row pitch of z32 (floats, multiple of 4)
+    float zmin32 = 0.0f;                            // lowest FP32 height of the DEM
     alignas(64) unsigned char tmap[sizeof(CUtensorMap)] = {};
     bool has_tmap = false;
 };
@@ -329,8 +330,13 @@ inline DemDev stage_dem(bsar_ctx* ctx, const bsar_dem* d, bool want_z32)
         // rows padded to a multiple of 4 floats: 16-byte tensor-map strides
         r.pitch = (int)((d->nx + 3) & ~int64_t(3));
         std::vector<float> zf((size_t)r.pitch * d->ny, 0.0f);
+        float zmin = INFINITY;
         for (int64_t j = 0; j < d->ny; j++)
-            for (int64_t i = 0; i < d->nx; i++) zf[j * r.pitch + i] = (float)d->z[j * d->nx + i];
+            for (int64_t i = 0; i < d->nx; i++) {
+                zf[j * r.pitch + i] = (float)d->z[j * d->nx + i];
+                zmin = std::min(zmin, zf[j * r.pitch + i]);
+            }
+        r.zmin32 = zmin;
         r.z32 = dev_upload(ctx, zf.data(), sizeof(float) * zf.size());
         sync(ctx);   // zf goes out of scope
         v.z32 = r.z32->as<float>();
@@ -698,6 +704,7 @@ inline MixedReq mixed_request(const Scene* s, const BpArgs& a, bool fp16, int32_
     r.off_x = s->off_x;
     r.off_y = s->off_y;
     r.start_band = mixed_start_band(s->dem.view);
+    r.zmin = s->dem.zmin32;
     return r;
 }
 
