@@ -23,7 +23,7 @@ _i64 = C.c_int64
 _i32 = C.c_int32
 
 STATUS = {0: "ok", 1: "invalid argument", 2: "HBM budget exceeded", 3: "device wait timed out",
-          4: "CUDA error", 5: "not found", 6: "unsupported", 7: "queue full"}
+          4: "CUDA error", 5: "not found", 6: "unsupported", 7: "queue full", 8: "cancelled"}
 SOLVER = {"grid": 0, "newton": 1}
 LEGS = {"mean": 0, "per_pulse": 1}
 PRECISION = {"fp64": 0, "mixed": 1, "mixed_fp16": 2}
@@ -73,7 +73,7 @@ class MatrixHeader(C.Structure):
 
 class ServerOpts(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_uint64), ("max_inflight", _i32), ("tiles_per_launch", _i32),
-                ("use_graph", _i32), ("reserved", _i32)]
+                ("use_graph", _i32), ("reserved", _i32), ("batch_timeout_s", C.c_double)]
 
 
 class Request(C.Structure):
@@ -117,6 +117,7 @@ def lib() -> C.CDLL:
         "bsar_set_stream": ([V, V], _i32),
         "bsar_synchronize": ([V], _i32),
         "bsar_launch_count": ([V], C.c_uint64),
+        "bsar_set_tile_wait_limit": ([V, _i64], _i32),
         "bsar_bytes_in_use": ([V], C.c_uint64),
         "bsar_dem_elevation": ([V, C.POINTER(Dem), _d, _i64, _d], _i32),
         "bsar_refraction_points": ([V, C.POINTER(Dem), _d, _d, _i64, C.c_double, C.c_double,
@@ -151,6 +152,7 @@ def lib() -> C.CDLL:
         "bsar_server_estimate": ([C.POINTER(Request), C.POINTER(C.c_uint64)], _i32),
         "bsar_server_poll": ([V, C.c_uint64, C.POINTER(_i32), _d], _i32),
         "bsar_server_wait": ([V, C.c_uint64, C.c_double, _d], _i32),
+        "bsar_server_cancel": ([V, C.c_uint64], _i32),
         "bsar_server_get_stats": ([V, C.POINTER(ServerStats)], _i32),
         "bsar_server_destroy": ([V], None),
     }
@@ -228,6 +230,10 @@ class Context:
     @property
     def launches(self) -> int:
         return int(self.L.bsar_launch_count(self.h))
+
+    def set_tile_wait_limit(self, polls: int) -> None:
+        """Polls of the mixed kernel's bounded DEM-tile wait (< 0: the default, 2^24)."""
+        self._ok(self.L.bsar_set_tile_wait_limit(self.h, int(polls)))
 
     @property
     def bytes_in_use(self) -> int:
@@ -460,12 +466,14 @@ class Server:
     ``submit`` copies the small arrays; the raw samples (if any) and the output image
     are kept alive here until the request completes."""
 
-    def __init__(self, ctx: Context, *, hbm_budget_bytes=0, max_inflight=64, tiles_per_launch=0, use_graph=True):
+    def __init__(self, ctx: Context, *, hbm_budget_bytes=0, max_inflight=64, tiles_per_launch=0, use_graph=True,
+                 batch_timeout_s=0.0):
         self.ctx = ctx
         self.L = ctx.L
         h = C.c_void_p()
         st = self.L.bsar_server_create(ctx.h, C.byref(ServerOpts(hbm_budget_bytes, max_inflight, tiles_per_launch,
-                                                                  1 if use_graph else 0, 0)), C.byref(h))
+                                                                  1 if use_graph else 0, 0, batch_timeout_s)),
+                                       C.byref(h))
         if st != 0:
             raise BsarError(st, ctx.last_error())
         self.h = h
@@ -528,6 +536,12 @@ class Server:
             raise BsarError(st, f"request {rid}")
         out, _ = self._live.pop(rid)
         return out, float(lat.value)
+
+    def cancel(self, rid: int) -> None:
+        """bsar_server_cancel: the request completes with BSAR_ERR_CANCELLED."""
+        st = self.L.bsar_server_cancel(self.h, rid)
+        if st != 0:
+            raise BsarError(st, f"cancel {rid}")
 
     def stats(self) -> dict:
         o = ServerStats()

@@ -22,6 +22,7 @@ const char* bsar_status_string(bsar_status s)
     case BSAR_ERR_NOT_FOUND: return "not found";
     case BSAR_ERR_UNSUPPORTED: return "unsupported";
     case BSAR_ERR_QUEUE_FULL: return "queue full";
+    case BSAR_ERR_CANCELLED: return "cancelled";
     }
     return "unknown status";
 }
@@ -492,10 +493,16 @@ static void backproject(bsar_ctx* ctx, bsar_scene_id id, const bsar_grid* g, con
     cuda_check(cudaMemcpyAsync(ctx->mixed_req->p, &r, sizeof r, cudaMemcpyHostToDevice, ctx->stream), "h2d");
     cuda_check(cudaMemsetAsync(ctx->mixed_counter->p, 0, sizeof(int), ctx->stream), "memset");
     MixedBatch b{ctx->mixed_req->as<MixedReq>(), nullptr, nullptr, (int)(vtiles * K),
-                 ctx->mixed_counter->as<int>(), ctx->status->as<int>(), chunks ? chunks->as<MixedChunks>() : nullptr};
+                 ctx->mixed_counter->as<int>(), ctx->status->as<int>(), chunks ? chunks->as<MixedChunks>() : nullptr,
+                 (long long)ctx->tile_wait_polls};
     const int grid = (int)std::min<int64_t>(b.ntiles, mixed_grid_ctas());
     cudaError_t e = launch_bp_mixed(b, a.W, grid, ctx->stream, K > 1);
     launched(ctx, e, "back-projection (mixed)");
+}
+
+bsar_status bsar_set_tile_wait_limit(bsar_ctx* ctx, int64_t polls)
+{
+    return guarded(ctx, [&] { ctx->tile_wait_polls = polls < 0 ? kDefaultTileWaitPolls : polls; });
 }
 
 bsar_status bsar_backproject(bsar_ctx* ctx, bsar_scene_id id, const bsar_grid* g, const bsar_bp_opts* o,

@@ -164,7 +164,8 @@ extern "C" bsar_status bsar_backproject_mixed_noalloc(bsar_ctx* ctx, bsar_scene_
         }
         MixedReq* d_req = reinterpret_cast<MixedReq*>(S + o_req);
         cuda_check(cudaMemcpyAsync(d_req, &r, sizeof r, cudaMemcpyHostToDevice, st), "request record");
-        MixedBatch b{d_req, nullptr, nullptr, (int)(vtiles * K), counter, status, d_chunks};
+        MixedBatch b{d_req, nullptr, nullptr, (int)(vtiles * K), counter, status, d_chunks,
+                     (long long)ctx->tile_wait_polls};
         const int grid = (int)std::min<int64_t>(b.ntiles, mixed_grid_ctas());
         launched(ctx, launch_bp_mixed(b, a.W, grid, st, K > 1), "back-projection (mixed, scratch)");
         cuda_check(cudaMemcpyAsync(image_out, a.out, 16 * (size_t)nv, cudaMemcpyDeviceToHost, st), "image");

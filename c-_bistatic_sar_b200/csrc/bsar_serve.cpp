@@ -33,7 +33,7 @@ using Clock = std::chrono::steady_clock;
 constexpr int kChunkedKey = 1 << 16;
 
 constexpr int kMaxSlots = 256;
-constexpr double kBatchTimeoutS = 300.0;   // bounded wait for one batch
+constexpr double kBatchTimeoutS = 300.0;   // default bound on the wait for one batch
 
 enum class St { Pending, Active, Done, Failed };
 
@@ -51,6 +51,7 @@ struct Req {
     double snr_db = 0;
     uint64_t seed = 0;
     double* image_out = nullptr;
+    bool cancelled = false;                         // bsar_server_cancel: no further work items
     // device state while admitted
     int slot = -1;
     uint64_t reserved = 0;
@@ -129,6 +130,8 @@ struct bsar_server {
     bool any_submit = false;
     Clock::time_point t_first, t_last;
     std::string fatal;
+    bsar_status fatal_status = BSAR_ERR_CUDA;       // what the requests left at a stop fail with
+    double batch_timeout_s = kBatchTimeoutS;
 };
 
 namespace {
@@ -311,7 +314,8 @@ cudaGraphExec_t batch_graph(bsar_server* s, ServeBatch& bt, int W)
     auto it = bt.graphs.find(W);
     if (it != bt.graphs.end()) return it->second;
     MixedBatch b{bt.d_reqs->as<MixedReq>(), bt.d_tiles->as<int2>(), bt.d_ntiles->as<int>(), 0,
-                 bt.d_counter->as<int>(), s->ctx->status->as<int>(), bt.d_chunks->as<MixedChunks>()};
+                 bt.d_counter->as<int>(), s->ctx->status->as<int>(), bt.d_chunks->as<MixedChunks>(),
+                 (long long)s->ctx->tile_wait_polls};
     cudaGraph_t g = nullptr;
     cuda_check(cudaStreamBeginCapture(bt.st, cudaStreamCaptureModeThreadLocal), "begin capture");
     cudaMemcpyAsync(bt.d_reqs->p, bt.h_reqs, sizeof(MixedReq) * kMaxSlots, cudaMemcpyHostToDevice, bt.st);
@@ -336,7 +340,7 @@ void launch_batch(bsar_server* s, ServeBatch& bt, int W, int n)
         cuda_check(cudaGraphLaunch(batch_graph(s, bt, W), bt.st), "graph launch");
     } else {
         MixedBatch b{bt.d_reqs->as<MixedReq>(), bt.d_tiles->as<int2>(), nullptr, n, bt.d_counter->as<int>(),
-                     s->ctx->status->as<int>(), bt.d_chunks->as<MixedChunks>()};
+                     s->ctx->status->as<int>(), bt.d_chunks->as<MixedChunks>(), (long long)s->ctx->tile_wait_polls};
         cuda_check(cudaMemcpyAsync(bt.d_reqs->p, bt.h_reqs, sizeof(MixedReq) * kMaxSlots, cudaMemcpyHostToDevice, bt.st),
                    "h2d");
         cuda_check(cudaMemcpyAsync(bt.d_chunks->p, bt.h_chunks, sizeof(MixedChunks) * kMaxSlots, cudaMemcpyHostToDevice,
@@ -392,6 +396,13 @@ bool admit_one(bsar_server* s, std::unique_lock<std::mutex>& lk)
     }
     if (st != BSAR_OK) release(s, r);
     lk.lock();
+    if (st == BSAR_OK && r->cancelled) {     // cancelled while being admitted
+        lk.unlock();
+        release(s, r);
+        lk.lock();
+        st = BSAR_ERR_CANCELLED;
+        err = "cancelled";
+    }
     if (st == BSAR_OK) {
         r->state = St::Active;
         s->active.push_back(r);
@@ -412,8 +423,10 @@ std::string wait_batch(bsar_server* s, ServeBatch& bt, std::unique_lock<std::mut
         cudaError_t e = cudaEventQuery(bt.ev);
         if (e == cudaSuccess) return std::string();
         if (e != cudaErrorNotReady) return std::string("batch: ") + cudaGetErrorString(e);
-        if (std::chrono::duration<double>(Clock::now() - t0).count() > kBatchTimeoutS)
+        if (std::chrono::duration<double>(Clock::now() - t0).count() > s->batch_timeout_s) {
+            s->fatal_status = BSAR_ERR_TIMEOUT;
             return "a batch did not finish within its time limit";
+        }
         if (!admit_one(s, lk)) {
             lk.unlock();
             std::this_thread::sleep_for(std::chrono::microseconds(50));
@@ -432,15 +445,21 @@ void retire_finished(bsar_server* s, std::unique_lock<std::mutex>& lk)
         lk.unlock();
         bsar_status st = BSAR_OK;
         std::string err;
-        try {
-            with_ctx(s, s->io, true, [&] {
-                cuda_check(cudaMemcpyAsync(r->image_out, r->image->p, r->image->bytes, cudaMemcpyDeviceToHost, s->io),
-                           "image d2h");
-                sync(s->ctx);
-            });
-        } catch (const Error& e) {
-            st = e.status;
-            err = e.msg;
+        if (r->cancelled) {
+            st = BSAR_ERR_CANCELLED;
+            err = "cancelled";
+        } else {
+            try {
+                with_ctx(s, s->io, true, [&] {
+                    cuda_check(cudaMemcpyAsync(r->image_out, r->image->p, r->image->bytes, cudaMemcpyDeviceToHost,
+                                               s->io),
+                               "image d2h");
+                    sync(s->ctx);
+                });
+            } catch (const Error& e) {
+                st = e.status;
+                err = e.msg;
+            }
         }
         release(s, r);
         lk.lock();
@@ -470,7 +489,9 @@ void worker_main(bsar_server* s)
         for (ServeBatch& bt : s->batch)
             if (bt.inflight && (!old || bt.seq < old->seq)) old = &bt;
         if (!old) {
-            // nothing on the device: admit, or sleep until work arrives
+            // nothing on the device: retire what needs no more work (cancelled requests),
+            // admit, or sleep until work arrives
+            retire_finished(s, lk);
             if (!admit_one(s, lk)) s->cv_work.wait_for(lk, std::chrono::milliseconds(2));
             continue;
         }
@@ -518,9 +539,10 @@ void worker_main(bsar_server* s)
     // fail whatever is left (device buffers are released by bsar_server_destroy after
     // the batch streams are synchronised)
     const std::string why = s->fatal.empty() ? "server stopped" : s->fatal;
-    for (Req* r : s->active) finish(s, r, BSAR_ERR_CUDA, why);
+    const bsar_status st = s->fatal.empty() ? BSAR_ERR_CUDA : s->fatal_status;
+    for (Req* r : s->active) finish(s, r, st, why);
     s->active.clear();
-    for (Req* r : s->pending) finish(s, r, BSAR_ERR_CUDA, why);
+    for (Req* r : s->pending) finish(s, r, st, why);
     s->pending.clear();
     s->cv_done.notify_all();
 }
@@ -548,6 +570,8 @@ bsar_status bsar_server_create(bsar_ctx* ctx, const bsar_server_opts* opts, bsar
     if (opts) s->opts = *opts;
     if (s->opts.max_inflight <= 0) s->opts.max_inflight = 64;
     if (s->opts.max_inflight > kMaxSlots) return BSAR_ERR_INVALID_ARG;
+    if (!(s->opts.batch_timeout_s >= 0.0)) return BSAR_ERR_INVALID_ARG;
+    if (s->opts.batch_timeout_s > 0.0) s->batch_timeout_s = s->opts.batch_timeout_s;
     std::lock_guard<std::mutex> lk(ctx->mu);
     try {
         cuda_check(cudaSetDevice(ctx->device), "cudaSetDevice");
@@ -652,7 +676,8 @@ bsar_status bsar_server_submit(bsar_server* s, const bsar_request* q, bsar_reque
     r->seed = q->seed;
     r->image_out = q->image_out;
     std::lock_guard<std::mutex> lk(s->mu);
-    if (s->stop || !s->fatal.empty()) return BSAR_ERR_CUDA;
+    if (s->stop) return BSAR_ERR_CUDA;
+    if (!s->fatal.empty()) return s->fatal_status;
     r->id = s->next_id++;
     r->t_submit = Clock::now();
     if (!s->any_submit) {
@@ -707,6 +732,29 @@ bsar_status bsar_server_wait(bsar_server* s, bsar_request_id id, double timeout_
     }
     if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count();
     return r->status;
+}
+
+bsar_status bsar_server_cancel(bsar_server* s, bsar_request_id id)
+{
+    if (!s) return BSAR_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(id);
+    if (it == s->reqs.end()) return BSAR_ERR_NOT_FOUND;
+    Req* r = it->second.get();
+    if (r->state == St::Done || r->state == St::Failed) return BSAR_ERR_NOT_FOUND;
+    r->cancelled = true;
+    auto p = std::find(s->pending.begin(), s->pending.end(), r);
+    if (p != s->pending.end()) {
+        s->pending.erase(p);
+        finish(s, r, BSAR_ERR_CANCELLED, "cancelled");
+        s->cv_done.notify_all();
+        return BSAR_OK;
+    }
+    // admitted (or being admitted): no further work items; the worker releases it when the
+    // items already on the device are done
+    if (r->state == St::Active) r->ntiles = r->next_tile;
+    s->cv_work.notify_all();
+    return BSAR_OK;
 }
 
 bsar_status bsar_server_get_stats(bsar_server* s, bsar_server_stats* o)

@@ -820,10 +820,12 @@ __device__ void drain_tile(uint64_t* mbar, uint32_t parity)
 }
 
 // Arms `mbar` and has one elected thread load the tile with a TMA 2-D tiled copy that
-// completes on it; every thread then waits (bounded) for the barrier's phase `parity`.
+// completes on it; every thread then waits for the barrier's phase `parity`, at most
+// `polls` polls (the draining wait before exit has its own fixed limit, kWaitSpins).
 // Returns false (and raises *status) if the copy did not complete in time.  The caller
 // has initialised the barrier and synchronised the CTA after the previous tile's readers.
-__device__ bool stage_tile(const void* tmap, float* tile, uint64_t* mbar, int i0, int j0, uint32_t parity, int* status)
+__device__ bool stage_tile(const void* tmap, float* tile, uint64_t* mbar, int i0, int j0, uint32_t parity, long long polls,
+                           int* status)
 {
     const uint32_t bar = smem_u32(mbar);
     if (threadIdx.x == 0) {
@@ -839,7 +841,7 @@ __device__ bool stage_tile(const void* tmap, float* tile, uint64_t* mbar, int i0
             : "memory");
     }
     uint32_t done = 0;
-    for (long s = 0; s < kWaitSpins && !done; s++) done = mbar_try_wait_parity(bar, parity);
+    for (long long s = 0; s < polls && !done; s++) done = mbar_try_wait_parity(bar, parity);
     if (!done && status) atomicExch(status, 1);
     return done != 0;
 }
@@ -1043,9 +1045,12 @@ __global__ void __launch_bounds__(128, 4) k_bp_mixed(MixedBatch b)
             const int ci = (int)floor((cx - m.ox) / m.stepx), cj = (int)floor((cy - m.oy) / m.stepy);
             T.i0 = ((ci - TI / 2) >> 2) << 2;      // TMA: x offset a multiple of 4 floats (16 B)
             T.j0 = cj - TJ / 2;
-            T.ok = stage_tile(R.tmap, tile_s, &mbar, T.i0, T.j0, parity, b.status);
+            const bool seen = stage_tile(R.tmap, tile_s, &mbar, T.i0, T.j0, parity, b.wait_polls, b.status);
             parity ^= 1u;
-            copy_pending = !T.ok;
+            // one view for the whole CTA: the tile is used only if every thread saw it land,
+            // and a copy is still in flight only if the thread that issued it did not
+            T.ok = __syncthreads_and(seen);
+            copy_pending = __syncthreads_or(threadIdx.x == 0 && !seen);
         }
         if constexpr (!CH) {
             voxel_mixed<WT, false>(a, m, T, table_buf, R.fp16 != 0, (int64_t)w.y * 128 + threadIdx.x, 0, 0,

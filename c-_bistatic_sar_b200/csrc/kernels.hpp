@@ -126,6 +126,7 @@ struct MixedBatch {
     int* counter;            // zeroed before the launch
     int* status;             // device status word (1 = a tile copy timed out)
     const MixedChunks* chunks;   // per request, indexed as reqs (the chunked kernel only)
+    long long wait_polls;        // polls of the bounded DEM-tile wait before giving up on a tile
 };
 
 cudaError_t launch_bp_plain(const BpArgs& a, int solver, int legs, cudaStream_t st);

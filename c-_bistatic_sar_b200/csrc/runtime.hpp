@@ -29,6 +29,7 @@ namespace bsar_rt {
 
 constexpr double kPi = 3.14159265358979323846;
 constexpr double kDefaultSearchRadius = 1.5;   // m, Newton node-scan radius
+constexpr int64_t kDefaultTileWaitPolls = int64_t(1) << 24;
 
 struct Error {
     bsar_status status;
@@ -99,6 +100,8 @@ struct bsar_ctx {
     // taken with `use_pool` cleared.
     cudaMemPool_t pool = nullptr;
     bool use_pool = false;
+    // polls of the mixed kernel's bounded DEM-tile wait (bsar_set_tile_wait_limit)
+    int64_t tile_wait_polls = kDefaultTileWaitPolls;
 };
 
 struct DevBuf {

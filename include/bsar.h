@@ -43,7 +43,8 @@ typedef enum bsar_status {
     BSAR_ERR_CUDA = 4,         /* a CUDA runtime error (message in bsar_last_error)  */
     BSAR_ERR_NOT_FOUND = 5,    /* unknown scene or request id                        */
     BSAR_ERR_UNSUPPORTED = 6,  /* a valid request outside what this build implements */
-    BSAR_ERR_QUEUE_FULL = 7    /* serving: no admission slot right now               */
+    BSAR_ERR_QUEUE_FULL = 7,   /* serving: no admission slot right now               */
+    BSAR_ERR_CANCELLED = 8     /* serving: the request was cancelled                 */
 } bsar_status;
 
 /* Fermat crossing-point solver. */
@@ -103,6 +104,14 @@ const char* bsar_last_error(const bsar_ctx* ctx);
 /* Use a caller-owned cudaStream_t for all work of this context (NULL = own stream). */
 bsar_status bsar_set_stream(bsar_ctx* ctx, void* cuda_stream);
 bsar_status bsar_synchronize(bsar_ctx* ctx);
+/* Bounded wait of the mixed kernel for its DEM tile copies (TMA): polls of the copy's
+ * barrier before a CTA gives up on the tile, reads the heights from global memory instead
+ * (the same values, so the same image) and raises the context's status word, which the
+ * call then reports as BSAR_ERR_TIMEOUT.  polls < 0 restores the default (2^24); 0 makes
+ * every wait run out at once, with no fault and no hang (the copy that was started is
+ * still waited for before the CTA exits).  Read when a launch is issued (a server reads
+ * it when it records a batch launch). */
+bsar_status bsar_set_tile_wait_limit(bsar_ctx* ctx, int64_t polls);
 /* Number of this library's kernel launches issued by the context so far. */
 uint64_t bsar_launch_count(const bsar_ctx* ctx);
 /* Device bytes currently held by the context (scenes, work buffers). */
@@ -344,6 +353,11 @@ typedef struct bsar_server_opts {
     int32_t tiles_per_launch;   /* work items per launch (0 = two waves of resident CTAs) */
     int32_t use_graph;          /* 1: every launch replays a captured CUDA graph           */
     int32_t reserved;
+    double batch_timeout_s;     /* host-side limit on one batch's device time (0 = 300 s);
+                                   when it runs out the server stops: the requests it holds
+                                   fail with BSAR_ERR_TIMEOUT and later submissions are
+                                   refused, and bsar_server_destroy still waits for the
+                                   batches on the device before it frees their memory     */
 } bsar_server_opts;
 
 typedef struct bsar_request {
@@ -384,6 +398,11 @@ bsar_status bsar_server_poll(bsar_server* srv, bsar_request_id id, int32_t* done
 /* Waits up to timeout_s (BSAR_ERR_TIMEOUT when it runs out). */
 bsar_status bsar_server_wait(bsar_server* srv, bsar_request_id id, double timeout_s, double* latency_ms);
 bsar_status bsar_server_get_stats(bsar_server* srv, bsar_server_stats* out);
+/* Cancels a request: a queued one is dropped at once, an admitted one gets no further
+ * work items and is released when the ones already on the device finish.  Either way it
+ * completes with BSAR_ERR_CANCELLED, its image_out untouched, and the other requests are
+ * unaffected.  BSAR_ERR_NOT_FOUND for unknown or already finished requests. */
+bsar_status bsar_server_cancel(bsar_server* srv, bsar_request_id id);
 void bsar_server_destroy(bsar_server* srv);
 
 #ifdef __cplusplus
