@@ -55,3 +55,17 @@ def backproject_sharded(compute, gx, gy, gz, dist=None):
         rb, re_ = z_slab(len(gz), r, world)
         full[:, :, rb:re_] = o.cpu().numpy().view(np.complex128)[:, :, : re_ - rb]
     return full
+
+
+def backproject_scene(ctx, sid, gx, gy, gz, dist=None, **opts):
+    """Image of scene `sid` with the grid's z axis split over the ranks of `dist` (strong
+    scaling): each rank back-projects its own contiguous z-slab on its own device through
+    ctx.backproject -- the reference's voxel loop (proc_test_script.cpp:451) cut into
+    ranges, no exchange while imaging -- and the slabs are gathered into the full image
+    (nx, ny, nz), z fastest, on every rank.  `opts` are ctx.backproject's keywords.
+
+    A voxel's value does not depend on which rank or slab computes it as long as the
+    pulse-chunk rule gives the slab and the full grid the same chunking (grids that fill
+    the GPU, or fewer than 256 pulses); then the gathered image equals a one-process run
+    bit for bit."""
+    return backproject_sharded(lambda x, y, z: ctx.backproject(sid, x, y, z, **opts), gx, gy, gz, dist)
