@@ -264,6 +264,8 @@ def parity_sample(sp, scat_voxel, seed: int, target: int = 3000):
     voxel belongs to (-1: lattice)."""
     rng = np.random.default_rng(seed)
     s = max(1, int(math.ceil((sp.n_voxels / target) ** (1.0 / 3.0))))
+    while math.prod(-(-n // s) for n in (sp.nx, sp.ny, sp.nz)) > target:     # thin grids: widen the stride
+        s += 1
     lat = [np.arange(rng.integers(0, min(s, n)), n, s) for n in (sp.nx, sp.ny, sp.nz)]
     ii = np.stack(np.meshgrid(*lat, indexing="ij"), axis=-1).reshape(-1, 3)
     groups = [np.full(len(ii), -1)]
@@ -328,6 +330,105 @@ def parity_block(ctx, sid, sc, ii, lat, hoods, groups, det, full_images, W):
             "mixed_fp16_vs_oracle": sample_stats(full_images["mixed_fp16"][at], orc, groups),
             "oracle_newton_cpu_s": t_orc,
             "bars": "FP64 forms rel-L2 <= 1e-9; mixed forms rel-L2 <= 1e-3, phase <= 0.01 rad; same argmax"}
+
+
+def config5_leg(ctx, torch, stream, nz: int = 8, steps: int = 2, cpu_voxels: int = 180, hoods: int = 4):
+    """The large scene (512 x 512 grid at 0.02 m, 2048 pulses, 16384 -> 65536 samples,
+    1024^2 fBm DEM at 0.125 m, so 25 x 25 node scans) on a z-slab of `nz` slices: pulse
+    compression + x4 upsampling and the mixed back-projection timed per step; the mixed
+    image against the GPU FP64 Newton image on one z-slice; mixed crossing points against
+    FP64; a CPU sample (uniform sub-lattice of the slab + the neighbourhoods of up to
+    `hoods` scatterers inside it) run by the reference's compiled code against the GPU
+    reference algorithm, and by the oracle's FP64 Newton against the GPU FP64 Newton and
+    mixed values.  Echoes are synthesised on the GPU."""
+    import bsar
+    from bsar import scene as S
+
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+
+    spec = S.scaled(S.config_spec(5), nz=nz)
+    sc = S.make_scene(spec, with_raw=False)
+    s0 = bsar.synthesize_scene(ctx, sc)
+    sc.raw = ctx.scene_read_samples(s0, spec.n_pulses, spec.n_samples)
+    ctx.scene_release(s0)
+    sid = bsar.upload_scene(ctx, sc)
+    W = S.search_nodes_for(sc.x_vec, sc.y_vec)
+    vp = spec.voxel_pulses
+    total_ms, bp_ms, img_mixed, _ = time_device(ctx, torch, stream, sid, sc, "mixed", "newton", "per_pulse", steps, 1)
+    pc_ms = [float(x) for x in time_device.pc_ms]
+    mixed = img_mixed.cpu().numpy().view(np.complex128).reshape(spec.nx, spec.ny, spec.nz)
+    del img_mixed
+    # FP64 Newton on the first z-slice of the slab
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    ref_slice = ctx.backproject(sid, sc.gx, sc.gy, sc.gz[:1], solver="newton", legs="per_pulse", precision="fp64")
+    torch.cuda.synchronize()
+    t64 = time.perf_counter() - t
+    mx = mixed[:, :, :1]
+    m = np.abs(ref_slice) >= 1e-3 * np.abs(ref_slice).max()
+    acc = {"mixed_vs_fp64_newton_slice": {
+        "voxels": int(ref_slice.size), "rel_l2": float(np.linalg.norm(mx - ref_slice) / np.linalg.norm(ref_slice)),
+        "max_phase_err_rad": float(np.abs(np.angle(mx[m] * np.conj(ref_slice[m]))).max()),
+        "argmax_match": bool(np.argmax(np.abs(mx)) == np.argmax(np.abs(ref_slice)))}}
+    # crossing points: mixed vs FP64 on random (pulse, voxel) pairs of the slab
+    rng = np.random.default_rng(0x5A4B0D5)
+    pi = rng.integers(0, spec.n_pulses, 1 << 14)
+    vi = rng.integers(0, [spec.nx, spec.ny, spec.nz], size=(1 << 14, 3))
+    P = np.stack([sc.gx[vi[:, 0]], sc.gy[vi[:, 1]], sc.gz[vi[:, 2]]], axis=1)
+    demA = bsar.DemArrays(sc.x_vec, sc.y_vec, sc.z)
+    cross = dpath = 0.0
+    for ant, na, nb, first in ((sc.tx, spec.n1, spec.n2, True), (sc.rx, spec.n2, spec.n1, False)):
+        p1, p2 = (ant[pi], P) if first else (P, ant[pi])
+        x64 = ctx.refraction_points(demA, p1, p2, na, nb, solver="newton")
+        x32 = ctx.refraction_points(demA, p1, p2, na, nb, solver="newton", precision="mixed")
+        cross = max(cross, float(np.linalg.norm(x32 - x64, axis=1).max()))
+        path = lambda X: na * np.linalg.norm(p1 - X, axis=1) + nb * np.linalg.norm(p2 - X, axis=1)  # noqa: E731
+        dpath = max(dpath, float(np.abs(path(x32) - path(x64)).max()))
+    acc["mixed_fermat_crossing_max_err_m"] = cross
+    acc["mixed_fermat_path_max_err_m"] = dpath
+    acc["fermat_sample"] = "16384 random (pulse, voxel) pairs per leg"
+    # CPU sample: the reference (grid search, mean legs) and the oracle's FP64 Newton
+    inside = [k for k, v in enumerate(sc.scat_voxel) if 1 <= v[2] <= spec.nz - 2][:hoods]
+    ii, lat, hd, groups = parity_sample(spec, sc.scat_voxel[inside], 0x5A4B0005, target=cpu_voxels)
+    threads = os.cpu_count() or 1
+    what = f"{len(ii)} sample voxels of the {spec.nz}-slice slab ({int((groups < 0).sum())} on a sub-lattice + " \
+           f"the 3x3x3 neighbourhoods of {len(hd)} scatterers)"
+    rate, det = cpu_reference_rate(sc, 0.0, threads, voxels=flat_voxels(spec, ii), what=what)
+    parts = [ctx.backproject(sid, sc.gx[lat[0]], sc.gy[lat[1]], sc.gz[lat[2]], solver="grid", legs="mean",
+                             precision="fp64").reshape(-1)]
+    parts64 = [ctx.backproject(sid, sc.gx[lat[0]], sc.gy[lat[1]], sc.gz[lat[2]], solver="newton", legs="per_pulse",
+                               precision="fp64").reshape(-1)]
+    for ax in hd:
+        parts.append(ctx.backproject(sid, sc.gx[ax[0]], sc.gy[ax[1]], sc.gz[ax[2]], solver="grid", legs="mean",
+                                     precision="fp64").reshape(-1))
+        parts64.append(ctx.backproject(sid, sc.gx[ax[0]], sc.gy[ax[1]], sc.gz[ax[2]], solver="newton",
+                                       legs="per_pulse", precision="fp64").reshape(-1))
+    orc = O.Oracle().backproject(O.Dem(sc.x_vec, sc.y_vec, sc.z), sc.tx, sc.rx, det["rc"], sc.gx, sc.gy, sc.gz,
+                                 spec.n1, spec.n2, 3e8, sc.fs_eff, sc.lam, legs="per_pulse", solver="newton",
+                                 voxels=flat_voxels(spec, ii), search_nodes=W)
+    at = (ii[:, 0], ii[:, 1], ii[:, 2])
+    acc["vs_cpu_sample"] = {
+        "voxels": int(len(ii)),
+        "fp64_grid_mean_vs_reference": sample_stats(np.concatenate(parts), det["values"], groups),
+        "fp64_newton_vs_oracle": sample_stats(np.concatenate(parts64), orc, groups),
+        "mixed_vs_oracle": sample_stats(mixed[at], orc, groups)}
+    ctx.scene_release(sid)
+    bp = statistics.mean(bp_ms)
+    ns = spec.n_samples
+    pc = statistics.median(pc_ms)
+    pc_bytes = spec.n_pulses * (16 * ns + 8 * ns * spec.upsample)
+    return {"workload": workload_name(spec) + f" (z-slab of {nz} slices)",
+            "voxel_pulses_per_s": vp / (total_ms / steps / 1e3), "ms_per_step": total_ms / steps,
+            "bp_kernel_ms": bp, "bp_voxel_pulses_per_s": vp / (bp / 1e3), "fermat_solves_per_s": 2 * vp / (bp / 1e3),
+            "node_scan_half_width": W,
+            "pulse_compression": {"ms": pc, "samples_per_s": spec.n_pulses * ns / (pc / 1e3),
+                                  "achieved_gbs": pc_bytes / (pc / 1e3) / 1e9},
+            "fp64_newton_slice_s": t64, "fp64_newton_voxel_pulses_per_s": ref_slice.size * spec.n_pulses / t64,
+            "accuracy": acc,
+            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": det["cores"], "kind": det["kind"],
+                             "sample": det["sample"]},
+            "steps": steps}
 
 
 def serve_leg(ctx, torch, n_requests: int, burst: int, fp64_sample: int, load: float = 0.8, tiles: int = 0):
@@ -478,6 +579,7 @@ def main():
     ap.add_argument("--serve-fp64-sample", type=int, default=24, help="requests run serially in FP64")
     ap.add_argument("--serve-only", action="store_true", help="only the served workload")
     ap.add_argument("--serve-tiles", type=int, default=0, help="work items per launch (0: two waves of CTAs)")
+    ap.add_argument("--no-config5", action="store_true", help="skip the large-scene slab leg")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -708,6 +810,10 @@ def main():
             cpu["as_shipped"] = {"value": r12, "cores": shipped,
                                  "note": "the reference caps its OpenMP loop at 12 threads"}
 
+    config5 = None
+    if rank == 0 and world == 1 and args.config == 2 and not args.no_config5 and not args.nz:
+        config5 = config5_leg(ctx, torch, stream)
+
     serving = None
     if rank == 0 and world == 1 and args.serve_requests > 0:
         ctx.set_stream(None)
@@ -736,6 +842,7 @@ def main():
             "cpu_baseline": cpu,
             "serving": serving,
             "strong_split": strong,
+            "config5": config5,
         }
         print(json.dumps(line), flush=True)
     ctx.scene_release(sid)
