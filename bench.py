@@ -529,6 +529,60 @@ def workload_name(sp) -> str:
             f"{sp.n_scatterers} scatterers, {sp.snr_db} dB")
 
 
+def kernel_tour():
+    """One launch of every library kernel on moderate sizes: the profiling case behind the
+    per-kernel summaries (inputs larger than L2 where a kernel streams memory)."""
+    import tempfile
+
+    import bsar
+    from bsar import scene as S
+
+    ctx = bsar.Context(0)
+    tmp = tempfile.mkdtemp()
+    # medium-scene signal and DEM on a 161 x 161 x 2 grid, 1024 pulses x 8192 samples
+    sp = S.scaled(S.config_spec(2), nz=2)
+    sc = S.make_scene(sp)
+    dem = bsar.DemArrays(sc.x_vec, sc.y_vec, sc.z)
+    sid = bsar.upload_scene(ctx, sc)
+    ctx.scene_compress(sid, "mixed")          # k_ref_spectrum<float>, k_pulse_compress_rf<13>
+    ctx.scene_compress(sid, "fp64")           # k_ref_spectrum<double>, k_pulse_compress<double>
+    ctx.backproject(sid, sc.gx, sc.gy, sc.gz, solver="newton", legs="per_pulse", precision="mixed")  # k_ref_ranges, k_bp_mixed
+    ctx.backproject(sid, sc.gx, sc.gy, sc.gz[:1], solver="newton", legs="per_pulse", precision="fp64")  # k_bp_plain<1,1>
+    ctx.backproject(sid, sc.gx, sc.gy[:60], sc.gz[:1], solver="grid", legs="mean", precision="fp64")  # k_bp_plain<0,0>
+    ctx.scene_release(sid)
+    ctx.scene_release(bsar.synthesize_scene(ctx, sc))           # k_echo_paths, k_echo_synth
+    # 16384-sample pulses in FP64: thread-block clusters (k_ref_spectrum_cl, k_pulse_compress_cl)
+    sc5 = S.make_scene(S.scaled(S.config_spec(5), n_pulses=256, nx=16, ny=16, nz=2))
+    s5 = bsar.upload_scene(ctx, sc5)
+    ctx.scene_compress(s5, "fp64")
+    ctx.scene_release(s5)
+    # pulse files in the simulator's row-major layout (k_transpose_c128), real-valued (k_real_to_c128)
+    raw = sc.raw[:256]
+    common = dict(n1=sp.n1, n2=sp.n2, fc=sp.fc, fs=sp.fs, chirp_f0=-sp.bandwidth / 2, chirp_f1=sp.bandwidth / 2,
+                  chirp_T=sp.pulse_T)
+    p1 = os.path.join(tmp, "raw.bin")
+    bsar.native.matrix_write(p1, np.ascontiguousarray(raw.T))
+    ctx.scene_release(ctx.scene_upload_file(dem, sc.tx[:256], sc.rx[:256], p1, layout="row_major", kind="raw",
+                                            **common))
+    p2 = os.path.join(tmp, "real.bin")
+    bsar.native.matrix_write(p2, np.ascontiguousarray(raw.real.T))
+    s4 = ctx.scene_upload_file(dem, sc.tx[:256], sc.rx[:256], p2, layout="row_major", kind="compressed", **common)
+    ctx.scene_compress(s4, "mixed")           # k_upsample_store
+    ctx.scene_compress(s4, "fp64")            # k_spline
+    ctx.scene_release(s4)
+    ctx.fft(sc.raw[:512])                     # k_fft_rows
+    rng = np.random.default_rng(3)
+    n = 1 << 16
+    P = np.stack([rng.uniform(19, 21, n), rng.uniform(-1.5, 1.5, n), rng.uniform(-6, -4, n)], 1)
+    A = sc.tx[rng.integers(0, sp.n_pulses, n)]
+    ctx.refraction_points(dem, A, P, sp.n1, sp.n2, solver="newton")                      # k_refraction_points<1>
+    ctx.refraction_points(dem, A, P, sp.n1, sp.n2, solver="newton", precision="mixed")   # k_refraction_mixed
+    ctx.dem_elevation(dem, P[:, :2])                                                      # k_dem_elevation
+    ctx.close()
+    print(json.dumps({"kernel_tour": "done"}), flush=True)
+    return 0
+
+
 def run_reference(args):
     """--impl reference: the reference's CPU implementation on the box's host cores."""
     rank = int(os.environ.get("RANK", "0"))
@@ -580,9 +634,12 @@ def main():
     ap.add_argument("--serve-only", action="store_true", help="only the served workload")
     ap.add_argument("--serve-tiles", type=int, default=0, help="work items per launch (0: two waves of CTAs)")
     ap.add_argument("--no-config5", action="store_true", help="skip the large-scene slab leg")
+    ap.add_argument("--kernel-tour", action="store_true", help="launch every kernel once (profiling case) and exit")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.kernel_tour:
+        return kernel_tour()
 
     import torch
 
