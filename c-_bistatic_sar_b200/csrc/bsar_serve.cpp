@@ -283,7 +283,6 @@ double request_deadline(const bsar_server* s, const Req* r)
 int build_batch(bsar_server* s, ServeBatch& b, int* W_out)
 {
     int n = 0, W = -1;
-    bool mixedW = false;
     std::vector<Req*> live;
     for (Req* r : s->active)
         if (r->next_tile < r->ntiles) live.push_back(r);
@@ -295,7 +294,12 @@ int build_batch(bsar_server* s, ServeBatch& b, int* W_out)
     std::vector<Item> list;
     std::map<Req*, int64_t> per_req;
     std::stable_sort(live.begin(), live.end(), [](const Req* x, const Req* y) { return x->deadline_s < y->deadline_s; });
+    // one node-scan width per batch, the earliest deadline's: each width runs its own kernel
+    // instantiation (the per-warp table scan), so a request's image does not depend on the
+    // widths of the requests it is batched with; other widths go to the next batch
+    const int W0 = live.front()->rec.a.W;
     for (Req* r : live) {
+        if (r->rec.a.W != W0) continue;
         const int64_t take = std::min<int64_t>(r->ntiles - r->next_tile, (int64_t)(s->max_tiles - n));
         // a work item's cost follows the pulses of its chunk
         const int cost = r->rec.a.np / std::max(1, r->chunks.nchunk);
@@ -304,8 +308,7 @@ int build_batch(bsar_server* s, ServeBatch& b, int* W_out)
             n += (int)take;
             r->next_tile += take;
             per_req[r] += take;
-            if (W < 0) W = r->rec.a.W;
-            else if (W != r->rec.a.W) mixedW = true;
+            W = W0;
         }
         if (n >= s->max_tiles) break;
     }
@@ -323,7 +326,7 @@ int build_batch(bsar_server* s, ServeBatch& b, int* W_out)
         if (per_req.count(r)) b.items.push_back({r, per_req[r]});
     bool chunked = false;
     for (const auto& it : b.items) chunked = chunked || it.first->chunks.nchunk > 1;
-    *W_out = (mixedW ? 0 : W) | (chunked ? kChunkedKey : 0);
+    *W_out = W | (chunked ? kChunkedKey : 0);
     return n;
 }
 

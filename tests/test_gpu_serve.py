@@ -167,3 +167,19 @@ def test_unsupported_precision_rejected_at_submit(ctx, mix):
         with pytest.raises(bsar.BsarError) as e:
             _submit(srv, mix.requests[0], precision="fp64")
         assert e.value.status == 6
+
+
+def test_requests_on_dems_of_different_spacing_share_the_server(ctx):
+    """Requests whose DEM spacings need different node-scan widths (0.25 m: 13 x 13 nodes,
+    0.5 m: 7 x 7) are in flight together; every image equals the one-request image."""
+    reqs = []
+    for k, (d, n) in enumerate([(0.25, 256), (0.5, 128), (0.25, 256), (0.5, 128)]):
+        spec = S.scaled(S.config_spec(2), nx=17, ny=15, nz=4, n_pulses=96, n_samples=2048, dem_d=d, dem_n=n,
+                        n_scatterers=3, seed=S.SEED_BASE + 300 + k)
+        reqs.append(S.make_scene(spec, with_raw=False))
+    assert {S.search_nodes_for(r.x_vec, r.y_vec) for r in reqs} == {3, 6}
+    with bsar.Server(ctx, max_inflight=4) as srv:
+        ids = [_submit(srv, sc) for sc in reqs]
+        imgs = [srv.wait(i)[0] for i in ids]
+    for sc, img in zip(reqs, imgs):
+        assert np.array_equal(img, _direct(ctx, sc, "mixed"))
