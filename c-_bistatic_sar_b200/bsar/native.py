@@ -139,6 +139,7 @@ def lib() -> C.CDLL:
         "bsar_scene_read_stored": ([V, C.c_uint64, _i32, _d], _i32),
         "bsar_backproject": ([V, C.c_uint64, C.POINTER(Grid), C.POINTER(BpOpts), _d], _i32),
         "bsar_backproject_device": ([V, C.c_uint64, C.POINTER(Grid), C.POINTER(BpOpts), V], _i32),
+        "bsar_backproject_range": ([V, C.c_uint64, C.POINTER(Grid), C.POINTER(BpOpts), _i64, _i64, _d], _i32),
         "bsar_backproject_mixed_noalloc": ([V, C.c_uint64, C.POINTER(Grid), C.POINTER(BpOpts), _d], _i32),
         "bsar_matrix_read_header": ([C.c_char_p, C.POINTER(MatrixHeader)], _i32),
         "bsar_matrix_read": ([C.c_char_p, _d, C.c_uint64], _i32),
@@ -386,6 +387,18 @@ class Context:
         elif out.shape != (g.nx, g.ny, g.nz) or out.dtype != np.complex128 or not out.flags.c_contiguous:
             raise ValueError("out must be a C-contiguous complex128 array of the grid's shape")
         self._ok(self.L.bsar_backproject(self.h, sid, C.byref(g), C.byref(o), _p(out.view(np.float64))))
+        return out
+
+    def backproject_range(self, sid: int, gx, gy, gz, v_begin: int, v_count: int, *, solver="grid", legs="mean",
+                          precision="fp64", search_radius_m=0.0, exhaustive=False):
+        """Voxels [v_begin, v_begin + v_count) of the grid's flat order (z -> x -> y) in the
+        full (nx, ny, nz) image, the others 0; each value equals backproject's."""
+        keep, g = self._grid(gx, gy, gz)
+        o = BpOpts(SOLVER[solver], LEGS[legs], PRECISION[precision], EXHAUSTIVE if exhaustive else 0,
+                   search_radius_m)
+        out = np.empty((g.nx, g.ny, g.nz), dtype=np.complex128)
+        self._ok(self.L.bsar_backproject_range(self.h, sid, C.byref(g), C.byref(o), int(v_begin), int(v_count),
+                                               _p(out.view(np.float64))))
         return out
 
     def backproject_mixed_noalloc(self, sid: int, gx, gy, gz, *, precision="mixed", search_radius_m=0.0,

@@ -59,13 +59,21 @@ def backproject_sharded(compute, gx, gy, gz, dist=None):
 
 def backproject_scene(ctx, sid, gx, gy, gz, dist=None, **opts):
     """Image of scene `sid` with the grid's z axis split over the ranks of `dist` (strong
-    scaling): each rank back-projects its own contiguous z-slab on its own device through
-    ctx.backproject -- the reference's voxel loop (proc_test_script.cpp:451) cut into
-    ranges, no exchange while imaging -- and the slabs are gathered into the full image
-    (nx, ny, nz), z fastest, on every rank.  `opts` are ctx.backproject's keywords.
+    scaling): each rank back-projects its own contiguous z-slab -- one range of the
+    reference's flat voxel loop (proc_test_script.cpp:451), through
+    ctx.backproject_range with the whole grid's per-pulse anchors -- on its own device,
+    with no exchange while imaging, and the slabs are gathered into the full image
+    (nx, ny, nz), z fastest, on every rank, equal bit for bit to a one-process run.
+    `opts` are ctx.backproject's keywords."""
+    nx, ny = len(gx), len(gy)
+    nz = len(gz)
 
-    A voxel's value does not depend on which rank or slab computes it as long as the
-    pulse-chunk rule gives the slab and the full grid the same chunking (grids that fill
-    the GPU, or fewer than 256 pulses); then the gathered image equals a one-process run
-    bit for bit."""
-    return backproject_sharded(lambda x, y, z: ctx.backproject(sid, x, y, z, **opts), gx, gy, gz, dist)
+    def slab(x, y, z_part):
+        # the slab's voxels are the range [b nx ny, e nx ny) of the full grid's order
+        world = dist.get_world_size() if dist else 1
+        rank = dist.get_rank() if dist else 0
+        b, e = z_slab(nz, rank, world)
+        full = ctx.backproject_range(sid, gx, gy, gz, b * nx * ny, (e - b) * nx * ny, **opts)
+        return full[:, :, b:e]
+
+    return backproject_sharded(slab, gx, gy, gz, dist)

@@ -428,10 +428,18 @@ static const double* stage_grid(bsar_ctx* ctx, const bsar_grid* g)
     return ctx->grid_dev->as<double>();
 }
 
-static void backproject(bsar_ctx* ctx, bsar_scene_id id, const bsar_grid* g, const bsar_bp_opts* o, double2* d_out)
+// The voxels [v_begin, v_begin + v_count) of the grid's flat order (v_count < 0: all) into
+// d_out, the full [x][y][z] image; per-pulse anchors and pulse chunks are those of the
+// whole grid, so a voxel's value does not depend on the range it is computed in.
+static void backproject(bsar_ctx* ctx, bsar_scene_id id, const bsar_grid* g, const bsar_bp_opts* o, double2* d_out,
+                        int64_t v_begin = 0, int64_t v_count = -1)
 {
     Scene* s = get_scene(ctx, id);
-    check_grid(g);
+    const int64_t nv_grid = check_grid(g);
+    if (v_count < 0) v_count = nv_grid - v_begin;
+    if (v_begin < 0 || v_count < 1 || v_begin > nv_grid - v_count)
+        fail(BSAR_ERR_INVALID_ARG, "voxel range [%lld, %lld) outside the grid's %lld voxels", (long long)v_begin,
+             (long long)(v_begin + v_count), (long long)nv_grid);
     if (!o) fail(BSAR_ERR_INVALID_ARG, "options are NULL");
     if (o->solver != BSAR_SOLVER_GRID && o->solver != BSAR_SOLVER_NEWTON) fail(BSAR_ERR_INVALID_ARG, "unknown solver");
     if (o->legs != BSAR_LEGS_MEAN && o->legs != BSAR_LEGS_PER_PULSE) fail(BSAR_ERR_INVALID_ARG, "unknown legs mode");
@@ -468,8 +476,8 @@ static void backproject(bsar_ctx* ctx, bsar_scene_id id, const bsar_grid* g, con
     a.fs_eff = s->fs * s->upsample;          // proc_test_script.cpp:220-223
     a.lambda = s->c / s->fc;                  // proc_test_script.cpp:213
     a.W = search_nodes(s->dem.view, o->search_radius_m);
-    a.v_begin = 0;
-    a.v_count = g->nx * g->ny * g->nz;
+    a.v_begin = v_begin;
+    a.v_count = v_count;
     a.out = d_out;
     if (o->precision == BSAR_FP64) {
         launched(ctx, launch_bp_plain(a, o->solver, o->legs, ctx->stream), "back-projection (FP64)");
@@ -481,7 +489,7 @@ static void backproject(bsar_ctx* ctx, bsar_scene_id id, const bsar_grid* g, con
     MixedReq r = mixed_request(s, a, o->precision == BSAR_MIXED_FP16, o->flags);
     // small grids: each tile's pulses in K chunks, so the work items fill the GPU
     const int64_t vtiles = (a.v_count + 127) / 128;
-    const int K = mixed_chunks(a.v_count, a.np);
+    const int K = mixed_chunks(nv_grid, a.np);
     std::unique_ptr<DevBuf> partial, tile_done, chunks;
     if (K > 1) {
         partial = dev_alloc(ctx, sizeof(double2) * (size_t)K * (size_t)(g->nx * g->ny * g->nz));
@@ -513,6 +521,21 @@ bsar_status bsar_backproject(bsar_ctx* ctx, bsar_scene_id id, const bsar_grid* g
         const int64_t nv = check_grid(g);
         auto img = dev_alloc(ctx, sizeof(double2) * nv);
         backproject(ctx, id, g, o, img->as<double2>());
+        cuda_check(cudaMemcpyAsync(image_out, img->p, sizeof(double2) * nv, cudaMemcpyDeviceToHost, ctx->stream), "d2h");
+        sync(ctx);
+        check_device_status(ctx);
+    });
+}
+
+bsar_status bsar_backproject_range(bsar_ctx* ctx, bsar_scene_id id, const bsar_grid* g, const bsar_bp_opts* o,
+                                   int64_t v_begin, int64_t v_count, double* image_out)
+{
+    return guarded(ctx, [&] {
+        if (!image_out) fail(BSAR_ERR_INVALID_ARG, "image_out is NULL");
+        const int64_t nv = check_grid(g);
+        auto img = dev_alloc(ctx, sizeof(double2) * nv);
+        cuda_check(cudaMemsetAsync(img->p, 0, sizeof(double2) * nv, ctx->stream), "clear image");
+        backproject(ctx, id, g, o, img->as<double2>(), v_begin, v_count);
         cuda_check(cudaMemcpyAsync(image_out, img->p, sizeof(double2) * nv, cudaMemcpyDeviceToHost, ctx->stream), "d2h");
         sync(ctx);
         check_device_status(ctx);

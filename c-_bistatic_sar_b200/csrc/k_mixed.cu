@@ -345,15 +345,10 @@ __device__ __forceinline__ AirTable build_air_table(const MixedCtx& m, const Til
 // Full (2W+1)^2 window inside the DEM and the warp table: height and E leg from the
 // table (one 8-byte load per node), the G leg per node, columns unrolled with
 // compile-time offsets.  The best node's row is updated once per row.
-// Out of line: it runs for the exhaustive flag and for warps whose lanes do not all have
-// full windows, so its body stays out of the pulse loop's instruction stream.
 template <int W>
-__device__ __noinline__ Rank scan_table(const MixedCtx m, const float2* tab, int ti0, int tj0, int is, int js, float gx,
-                                        float gy, float gz, Rank rk)
+__device__ __forceinline__ void scan_table_inl(const MixedCtx& m, const AirTable& AT, int is, int js, float gx,
+                                               float gy, float gz, float& v1, float& v2, int& bi, int& bj)
 {
-    float v1 = rk.v1, v2 = rk.v2;
-    int bi = rk.bi, bj = rk.bj;
-    const AirTable AT{const_cast<float2*>(tab), ti0, tj0, true};
     constexpr int NJ = 2 * W + 1;
     float syg[NJ];
 #pragma unroll
@@ -384,7 +379,18 @@ __device__ __noinline__ Rank scan_table(const MixedCtx m, const float2* tab, int
         bi = (v1 < v1_row) ? i : bi;
     }
     bj = js - W + bc;
-    return Rank{v1, v2, bi, bj};
+}
+
+// Out of line for the widths that prune: it runs for the exhaustive flag and for warps
+// whose lanes do not all have full windows, so its body stays out of the pulse loop's
+// instruction stream.
+template <int W>
+__device__ __noinline__ Rank scan_table(const MixedCtx m, const float2* tab, int ti0, int tj0, int is, int js, float gx,
+                                        float gy, float gz, Rank rk)
+{
+    const AirTable AT{const_cast<float2*>(tab), ti0, tj0, true};
+    scan_table_inl<W>(m, AT, is, js, gx, gy, gz, rk.v1, rk.v2, rk.bi, rk.bj);
+    return rk;
 }
 
 // Columns of a window row in groups of four for the pruned scan; a trailing single column
@@ -523,6 +529,9 @@ __device__ __forceinline__ void scan_pruned(const MixedCtx& m, const AirTable& A
     bj = js - W + bc;
 }
 
+// Narrowest node-scan half width whose table scan is pruned.
+constexpr int kPruneMinW = 6;
+
 template <int W, bool TABLE>
 __device__ __forceinline__ void node_scan(const MixedCtx& m, const Tile& T, const AirTable& AT, int is, int js, int Wr,
                                           const float E[3], const float G[3], float re, float tie, int seed, float& v1,
@@ -531,7 +540,14 @@ __device__ __forceinline__ void node_scan(const MixedCtx& m, const Tile& T, cons
     const int ia = max(is - Wr, 0), ib = min(is + Wr, m.nx - 1);
     const int ja = max(js - Wr, 0), jb = min(js + Wr, m.ny - 1);
     const bool in_tile = T.ok && ia >= T.i0 && ib < T.i0 + TI && ja >= T.j0 && jb < T.j0 + TJ;
-    if constexpr (W > 0 && TABLE) {
+    if constexpr (W > 0 && W < kPruneMinW && TABLE) {
+        // small windows: every node, inline (the bound tests would cost more than they save)
+        if (AT.ok && Wr == W && ia == is - W && ib == is + W && ja == js - W && jb == js + W) {
+            scan_table_inl<W>(m, AT, is, js, G[0], G[1], G[2], v1, v2, bi, bj);
+            return;
+        }
+    }
+    if constexpr (W >= kPruneMinW && TABLE) {
         const bool full_window = AT.ok && Wr == W && ia == is - W && ib == is + W && ja == js - W && jb == js + W;
         // the pruned scan votes across the warp: only when every lane takes it
         const bool all_full = __all_sync(0xffffffffu, full_window);

@@ -255,6 +255,16 @@ enum { BSAR_BP_EXHAUSTIVE_SCAN = 1 };
 bsar_status bsar_backproject(bsar_ctx* ctx, bsar_scene_id scene, const bsar_grid* grid,
                              const bsar_bp_opts* opts, double* image_out);
 
+/* A range of the imager's voxel loop: the voxels [v_begin, v_begin + v_count) of the
+ * grid's flat order (z -> x -> y, y fastest; proc_test_script.cpp:132-151, the index the
+ * OpenMP loop of :451 splits), written at their places in image_out, the full complex
+ * nx x ny x nz image [x][y][z]; every other voxel is set to 0.  Per-pulse anchors and
+ * pulse chunks are the whole grid's, so every voxel's value equals bsar_backproject's,
+ * bit for bit: ranges computed on several devices add up to the one-device image (a
+ * z-slab is one contiguous range). */
+bsar_status bsar_backproject_range(bsar_ctx* ctx, bsar_scene_id scene, const bsar_grid* grid,
+                                   const bsar_bp_opts* opts, int64_t v_begin, int64_t v_count, double* image_out);
+
 /* As bsar_backproject, but asynchronous on the context stream with the image written to
  * device memory d_image (complex128, same layout); the grid axes are read at the call. */
 bsar_status bsar_backproject_device(bsar_ctx* ctx, bsar_scene_id scene, const bsar_grid* grid,

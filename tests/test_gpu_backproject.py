@@ -121,6 +121,33 @@ def test_pruned_node_scan_is_bit_identical(ctx, which, precision, request):
     assert np.array_equal(pruned, full)
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("which", ["chunked", "rough"])
+def test_voxel_ranges_add_up_to_the_image(ctx, which, precision, request):
+    """bsar_backproject_range: three ranges of the flat voxel order, each with the whole
+    grid's anchors and pulse chunks, add up to bsar_backproject's image bit for bit."""
+    sc = request.getfixturevalue(which)
+    kw = dict(solver="newton", legs="per_pulse", precision=precision)
+    nv = len(sc.gx) * len(sc.gy) * len(sc.gz)
+    cuts = [0, nv // 3, (2 * nv) // 3 + 5, nv]
+    sid = bsar.upload_scene(ctx, sc)
+    try:
+        full = ctx.backproject(sid, sc.gx, sc.gy, sc.gz, **kw)
+        parts = [ctx.backproject_range(sid, sc.gx, sc.gy, sc.gz, a, b - a, **kw) for a, b in zip(cuts, cuts[1:])]
+        with pytest.raises(bsar.BsarError):
+            ctx.backproject_range(sid, sc.gx, sc.gy, sc.gz, nv - 3, 5, **kw)
+    finally:
+        ctx.scene_release(sid)
+    assert np.array_equal(parts[0] + parts[1] + parts[2], full)
+    flat = np.zeros(nv, dtype=bool)
+    flat[cuts[1]:cuts[2]] = True
+    zi, rem = np.divmod(np.arange(nv), len(sc.gx) * len(sc.gy))
+    xi, yi = np.divmod(rem, len(sc.gy))
+    mask = np.zeros(full.shape, dtype=bool)
+    mask[xi[flat], yi[flat], zi[flat]] = True
+    assert np.all(parts[1][~mask] == 0) and np.array_equal(parts[1][mask], full[mask])
+
+
 def test_unknown_backprojection_flags_are_rejected(ctx, small):
     sid = bsar.upload_scene(ctx, small)
     try:
