@@ -1017,10 +1017,18 @@ __device__ __forceinline__ void reduce_chunks(const BpArgs& a, const double2* __
 // CH: the instantiation for batches holding small-grid requests whose tiles run in pulse
 // chunks (MixedChunks); the last chunk of a tile to finish adds the chunks' sums in chunk
 // order.  Batches without chunks run the other instantiation, which never reads them.
+// The DEM tile is staged only for wide node scans (WT = 12, and the generic width): a
+// 25 x 25 scan builds 30-row warp tables every pulse and reads them from the tile faster
+// than through L1.  For 7 x 7 and 13 x 13 scans the tile's bookkeeping costs registers
+// (twice the spills) and its 17 KB per CTA shrinks L1, and the kernel runs faster with the
+// heights read from global memory -- the same FP32 values, so the same image.
+template <int WT> struct StagesTile { static constexpr bool v = WT == 0 || WT >= 12; };
+
 template <int WT, bool CH>
 __global__ void __launch_bounds__(128, 4) k_bp_mixed(MixedBatch b)
 {
-    __shared__ alignas(128) float tile_s[TI * TJ];
+    constexpr bool kTile = StagesTile<WT>::v;
+    __shared__ alignas(128) float tile_s[kTile ? TI * TJ : 32];
     __shared__ alignas(16) float2 air_s[4][TableRows<WT>::v * TBJ];   // one (z, E-leg) table per warp
     __shared__ alignas(8) uint64_t mbar;
     __shared__ int2 work;
@@ -1051,7 +1059,7 @@ __global__ void __launch_bounds__(128, 4) k_bp_mixed(MixedBatch b)
         const int tile = CH ? w.y / K : w.y;
         const int chunk = CH ? w.y - tile * K : 0;
         Tile T{tile_s, 0, 0, false};
-        if (R.use_tile && !copy_pending) {
+        if (kTile && R.use_tile && !copy_pending) {
             // DEM tile centred on this work item's voxels plus the mean crossing offset
             const int64_t v0 = a.v_begin + (int64_t)tile * 128;
             const int64_t vl = min(v0 + 128, a.v_begin + a.v_count) - 1;

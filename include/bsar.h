@@ -14,8 +14,8 @@
  *   - Host buffers are caller-owned and only read / written during the call; device
  *     memory is owned by the context.  The context takes it from its own stream-ordered
  *     pool (cudaMallocFromPoolAsync on the context's stream), which keeps freed blocks
- *     for later calls until bsar_destroy; bsar_bytes_in_use counts the live buffers.  Every call is synchronous unless its name ends
- *     in _device.
+ *     for later calls until bsar_destroy; bsar_bytes_in_use counts the live buffers.
+ *     Every call is synchronous unless its name ends in _device.
  *   - Every entry point returns a bsar_status; bsar_last_error(ctx) gives the message of
  *     the calling thread's latest call on ctx (empty after a success), so threads that
  *     share a context each read their own failure.  The string stays valid until that
@@ -104,13 +104,15 @@ const char* bsar_last_error(const bsar_ctx* ctx);
 /* Use a caller-owned cudaStream_t for all work of this context (NULL = own stream). */
 bsar_status bsar_set_stream(bsar_ctx* ctx, void* cuda_stream);
 bsar_status bsar_synchronize(bsar_ctx* ctx);
-/* Bounded wait of the mixed kernel for its DEM tile copies (TMA): polls of the copy's
- * barrier before a CTA gives up on the tile, reads the heights from global memory instead
- * (the same values, so the same image) and raises the context's status word, which the
- * call then reports as BSAR_ERR_TIMEOUT.  polls < 0 restores the default (2^24); 0 makes
- * every wait run out at once, with no fault and no hang (the copy that was started is
- * still waited for before the CTA exits).  Read when a launch is issued (a server reads
- * it when it records a batch launch). */
+/* Bounded wait of the mixed kernel for its DEM tile copies (TMA).  Node scans of half
+ * width 12, and of widths without a kernel of their own, stage a tile; the 3 and 6 scans
+ * read the DEM from global memory.  polls: polls of the copy's barrier before a CTA gives
+ * up on the tile, reads the heights from global memory instead (the same values, so the
+ * same image) and raises the context's status word, which the call then reports as
+ * BSAR_ERR_TIMEOUT.  polls < 0 restores the default (2^24); 0 makes every wait run out
+ * at once, with no fault and no hang (the copy that was started is still waited for
+ * before the CTA exits).  Read when a launch is issued (a server reads it when it records
+ * a batch launch). */
 bsar_status bsar_set_tile_wait_limit(bsar_ctx* ctx, int64_t polls);
 /* Number of this library's kernel launches issued by the context so far. */
 uint64_t bsar_launch_count(const bsar_ctx* ctx);

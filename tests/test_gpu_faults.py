@@ -4,7 +4,7 @@ that runs out by design, or a request the caller withdraws.
 * the mixed kernel's bounded wait for its DEM tile copy (limit 0: every wait runs out at
   once) reports BSAR_ERR_TIMEOUT, and the image is still the tiled run's, bit for bit,
   because the fallback reads the same heights from global memory; the next call with the
-  default limit succeeds;
+  default limit succeeds (a 25 x 25 node scan, the width whose kernel stages the tile);
 * a server whose batch time limit is shorter than any batch stops: its requests fail with
   BSAR_ERR_TIMEOUT, later submissions are refused, destroying it waits for the batch on
   the device, and the context serves a new server normally afterwards;
@@ -47,22 +47,23 @@ def _direct(ctx, sc):
         ctx.scene_release(sid)
 
 
+# 3 m on the 0.25 m DEM: 12 nodes each side
+WIDE = dict(solver="newton", legs="per_pulse", precision="mixed", search_radius_m=3.0)
+
+
 def test_tile_wait_that_runs_out_reports_timeout_with_the_same_image(scene):
     with bsar.Context(0) as ctx:
         sid = bsar.upload_scene(ctx, scene)
         try:
-            ref = ctx.backproject(sid, scene.gx, scene.gy, scene.gz, solver="newton", legs="per_pulse",
-                                  precision="mixed")
+            ref = ctx.backproject(sid, scene.gx, scene.gy, scene.gz, **WIDE)
             ctx.set_tile_wait_limit(0)
             out = np.zeros_like(ref)
             with pytest.raises(bsar.BsarError) as e:
-                ctx.backproject(sid, scene.gx, scene.gy, scene.gz, solver="newton", legs="per_pulse",
-                                precision="mixed", out=out)
+                ctx.backproject(sid, scene.gx, scene.gy, scene.gz, out=out, **WIDE)
             assert e.value.status == TIMEOUT
             assert np.array_equal(out, ref)
             ctx.set_tile_wait_limit(-1)
-            again = ctx.backproject(sid, scene.gx, scene.gy, scene.gz, solver="newton", legs="per_pulse",
-                                    precision="mixed")
+            again = ctx.backproject(sid, scene.gx, scene.gy, scene.gz, **WIDE)
             assert np.array_equal(again, ref)
         finally:
             ctx.scene_release(sid)
