@@ -49,9 +49,9 @@ sys.path.insert(0, str(ROOT / "c-_bistatic_sar_b200"))
 
 METRIC = "BP voxel-pulses/s (Fermat incl.), mixed vs FP64 @<=1e-3 rel-L2; served p99 ms"
 # DRAM bytes (read + write) of one k_bp_mixed launch on the full medium scene: a one-pass
-# ncu capture of dram__bytes_read.sum + dram__bytes_write.sum of the headline command with
-# the pruned node scan (4.67 MB + 5.51 MB); the pruning does not change the gathers
-TRAFFIC_BYTES = {2: 1.018e7}
+# ncu capture of dram__bytes_read.sum + dram__bytes_write.sum of the headline command
+# (4.18 MB + 2.46 MB; the gathers hit L2, and the image leaves L2 after the kernel ends)
+TRAFFIC_BYTES = {2: 6.64e6}
 UNIT = "voxel-pulses/s"
 
 
