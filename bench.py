@@ -490,7 +490,8 @@ def serve_leg(ctx, torch, n_requests: int, burst: int, fp64_sample: int, load: f
                      "seconds": wall, "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
                      "mean_ms": float(lat.mean()), "max_ms": float(lat.max()), "launches": int(st["launches"]),
                      "tiles": int(st["tiles"]), "peak_inflight": int(st["peak_inflight"]),
-                     "peak_reserved_gb": st["peak_reserved_bytes"] / 1e9, "failed": int(st["failed"])}
+                     "peak_reserved_gb": st["peak_reserved_bytes"] / 1e9, "failed": int(st["failed"]),
+                     "batch_busy_fraction": st["batch_busy_s"] / wall}
     # a request cannot finish sooner than its own work at the full measured capacity
     floor_ms = np.sort(vp / cap_vps * 1e3)
     out["served"]["p99_service_floor_ms"] = float(np.percentile(floor_ms, 99))

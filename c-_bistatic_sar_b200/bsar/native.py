@@ -86,7 +86,8 @@ class ServerStats(C.Structure):
     _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
                 ("launches", C.c_uint64), ("tiles", C.c_uint64), ("p50_ms", C.c_double), ("p99_ms", C.c_double),
                 ("mean_ms", C.c_double), ("max_ms", C.c_double), ("voxel_pulses", C.c_double),
-                ("busy_s", C.c_double), ("peak_inflight", C.c_uint64), ("peak_reserved_bytes", C.c_uint64)]
+                ("busy_s", C.c_double), ("peak_inflight", C.c_uint64), ("peak_reserved_bytes", C.c_uint64),
+                ("batch_busy_s", C.c_double)]
 
 
 def build(quiet: bool = True) -> Path:

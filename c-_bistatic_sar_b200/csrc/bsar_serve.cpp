@@ -126,6 +126,7 @@ struct bsar_server {
     Clock::time_point t_start = Clock::now();
     double rate_est = 1e9;                          // voxel-pulses/s of recent batches
     Clock::time_point t_last_batch_done = Clock::now();
+    double batch_busy_s = 0.0;                      // time with a batch on the device
     uint64_t batch_seq = 0;
     cudaStream_t io = nullptr;
     int grid_ctas = 0, max_tiles = 0;
@@ -563,6 +564,7 @@ void worker_main(bsar_server* s)
             const auto from = std::max(old->t_launch, s->t_last_batch_done);
             const double dt = std::chrono::duration<double>(now - from).count();
             if (dt > 1e-4 && old->voxel_pulses > 0) s->rate_est = 0.8 * s->rate_est + 0.2 * (old->voxel_pulses / dt);
+            if (dt > 0) s->batch_busy_s += dt;    // the intervals [from, now] do not overlap
             s->t_last_batch_done = now;
         }
         for (auto& p : old->items) p.first->done_tiles += p.second;
@@ -812,6 +814,7 @@ bsar_status bsar_server_get_stats(bsar_server* s, bsar_server_stats* o)
     o->busy_s = s->completed ? std::chrono::duration<double>(s->t_last - s->t_first).count() : 0.0;
     o->peak_inflight = s->peak_inflight;
     o->peak_reserved_bytes = s->peak_reserved;
+    o->batch_busy_s = s->batch_busy_s;
     return BSAR_OK;
 }
 

@@ -761,44 +761,72 @@ __device__ __forceinline__ double solve_mixed(const DemView& d, const MixedCtx& 
     }
     seed = (bi < 32768 && bj < 65536) ? (bi << 16) | bj : -1;
     // 3. polish the facets around the best node (FP32); heights from the DEM tile when the
-    //    node's 3 x 3 neighbourhood lies in it
+    //    node's 3 x 3 neighbourhood lies in it.  The nine heights are loaded once (indices
+    //    clamped to the DEM; a facet that would need a clamped one is not polished), and the
+    //    path's gradient at the node is formed once: with G = na (N - A)/|N - A| +
+    //    nb (N - B)/|N - B|, a facet with the node at its corner (u0, v0) has the gradient
+    //    (Gx + Gz zx, Gy + Gz zy), zx and zy the facet's slopes along the edges through the
+    //    node (one-sided differences: backward where u0 = 1, forward where u0 = 0).  When it
+    //    points out of the facet on both axes, the corner is that facet's minimum and the
+    //    facet keeps the node's path; the others take the Newton steps.
     const bool nt = T.ok && bi - 1 >= T.i0 && bi + 1 < T.i0 + TI && bj - 1 >= T.j0 && bj + 1 < T.j0 + TJ;
     auto zt = [&](int i, int j) { return nt ? T.s[(j - T.j0) * TI + (i - T.i0)] : zf(m, i, j); };
-    float Lnode;
+    const int im = max(bi - 1, 0), ip = min(bi + 1, m.nx - 1);
+    const int jm = max(bj - 1, 0), jp = min(bj + 1, m.ny - 1);
+    const float zmm = zt(im, jm), zm0 = zt(im, bj), zmp = zt(im, jp);
+    const float z0m = zt(bi, jm), z00n = zt(bi, bj), z0p = zt(bi, jp);
+    const float zpm = zt(ip, jm), zp0 = zt(ip, bj), zpp = zt(ip, jp);
+    float Lnode, gxb, gxf, gyb, gyf;
     {
-        float xn = (float)bi * m.stepx, yn = (float)bj * m.stepy, zn = zt(bi, bj);
-        float r1x = xn - A32[0], r1y = yn - A32[1], r1z = zn - A32[2];
-        float r2x = xn - B32[0], r2y = yn - B32[1], r2z = zn - B32[2];
+        float xn = (float)bi * m.stepx, yn = (float)bj * m.stepy;
+        float r1x = xn - A32[0], r1y = yn - A32[1], r1z = z00n - A32[2];
+        float r2x = xn - B32[0], r2y = yn - B32[1], r2z = z00n - B32[2];
         float q1 = r1x * r1x + r1y * r1y + r1z * r1z, q2 = r2x * r2x + r2y * r2y + r2z * r2z;
-        Lnode = na * (q1 * rsqrtf(q1)) + nb * (q2 * rsqrtf(q2));
+        const float s1 = rsqrtf(q1), s2 = rsqrtf(q2);
+        Lnode = na * (q1 * s1) + nb * (q2 * s2);
+        const float g1 = na * s1, g2 = nb * s2;
+        const float Gx = g1 * r1x + g2 * r2x, Gy = g1 * r1y + g2 * r2y, Gz = g1 * r1z + g2 * r2z;
+        gxb = fmaf(Gz, (z00n - zm0) * m.istepx, Gx);
+        gxf = fmaf(Gz, (zp0 - z00n) * m.istepx, Gx);
+        gyb = fmaf(Gz, (z00n - z0m) * m.istepy, Gy);
+        gyf = fmaf(Gz, (z0p - z00n) * m.istepy, Gy);
     }
     int bfi = min(bi, m.nx - 2), bfj = min(bj, m.ny - 2);     // fallback facet
     float bestF = INFINITY, bu = (float)(bi - bfi), bv = (float)(bj - bfj);
 #pragma unroll 1
     for (int k = 0; k < 4; k++) {
-        int fi = bi - 1 + (k >> 1), fj = bj - 1 + (k & 1);
+        const bool kx = k >> 1, ky = k & 1;       // facet on the +x / +y side of the node
+        int fi = bi - 1 + kx, fj = bj - 1 + ky;
         if (fi < 0 || fj < 0 || fi > m.nx - 2 || fj > m.ny - 2) continue;
-        Facet32 F;
-        F.x0 = (float)fi * m.stepx;
-        F.y0 = (float)fj * m.stepy;
-        F.dx = m.stepx;
-        F.dy = m.stepy;
-        F.idx = m.istepx;
-        F.idy = m.istepy;
-        float z00 = zt(fi, fj), z01 = zt(fi + 1, fj), z10 = zt(fi, fj + 1), z11 = zt(fi + 1, fj + 1);
-        F.z00 = z00;
-        F.b = z01 - z00;
-        F.c = z10 - z00;
-        F.e = z11 - z01 - z10 + z00;
         float u = (float)(bi - fi), v = (float)(bj - fj);
-        bool moved = false;
+        float L = Lnode;
+        const bool corner = (kx ? gxf > 0.0f : gxb < 0.0f) && (ky ? gyf > 0.0f : gyb < 0.0f);
+        if (!corner) {
+            Facet32 F;
+            F.x0 = (float)fi * m.stepx;
+            F.y0 = (float)fj * m.stepy;
+            F.dx = m.stepx;
+            F.dy = m.stepy;
+            F.idx = m.istepx;
+            F.idy = m.istepy;
+            // corners (fi, fj), (fi + 1, fj), (fi, fj + 1), (fi + 1, fj + 1) of the 3 x 3 block
+            const float z00 = kx ? (ky ? z00n : z0m) : (ky ? zm0 : zmm);
+            const float z01 = kx ? (ky ? zp0 : zpm) : (ky ? z00n : z0m);
+            const float z10 = kx ? (ky ? z0p : z00n) : (ky ? zmp : zm0);
+            const float z11 = kx ? (ky ? zpp : zp0) : (ky ? z0p : z00n);
+            F.z00 = z00;
+            F.b = z01 - z00;
+            F.c = z10 - z00;
+            F.e = z11 - z01 - z10 + z00;
+            bool moved = false;
 #pragma unroll 1
-        for (int it = 0; it < kPolishIters; it++) {
-            if (!facet_step32(F, A32, B32, na, nb, u, v)) break;
-            moved = true;
+            for (int it = 0; it < kPolishIters; it++) {
+                if (!facet_step32(F, A32, B32, na, nb, u, v)) break;
+                moved = true;
+            }
+            // a facet whose corner is already its minimum keeps the best node's path
+            if (moved) L = facet_eval32(F, A32, B32, na, nb, u, v);
         }
-        // a facet whose corner is already its minimum keeps the best node's path
-        float L = moved ? facet_eval32(F, A32, B32, na, nb, u, v) : Lnode;
         if (L < bestF) {
             bestF = L;
             bu = u;

@@ -393,6 +393,8 @@ typedef struct bsar_server_stats {
     double busy_s;                            /* first submission -> last completion */
     uint64_t peak_inflight;                   /* most requests admitted at once  */
     uint64_t peak_reserved_bytes;             /* most HBM reserved at once       */
+    double batch_busy_s;                      /* time with a batch on the device, as the
+                                                 server thread sees launches and completions */
 } bsar_server_stats;
 
 /* The server keeps `ctx` for itself until bsar_server_destroy (other calls on the same

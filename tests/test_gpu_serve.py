@@ -60,6 +60,8 @@ def test_same_alone_and_in_mix(served):
     assert np.array_equal(alone, imgs[0])
     assert st["completed"] == 7 and st["failed"] == 0
     assert st["peak_inflight"] >= 2
+    # batches were on the device for part of the span from first submission to last image
+    assert 0 < st["batch_busy_s"] <= st["busy_s"] + 1e-3
 
 
 def test_served_equals_one_request_entry_point(ctx, mix, served):
