@@ -117,6 +117,29 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------------------------
+def l2_copy_gbs(torch, stream, mib: int = 32, reps: int = 50) -> float:
+    """L2 bandwidth of this GPU, measured: a device copy between two buffers of `mib` MiB
+    (both resident in the 126 MB L2 after the first pass), read + write bytes over the
+    CUDA-event time of `reps` back-to-back copies, best of 5."""
+    n = mib * (1 << 20) // 4
+    a = torch.ones(n, dtype=torch.float32, device="cuda")
+    b = torch.empty_like(a)
+    best = 0.0
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            b.copy_(a)
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                b.copy_(a)
+            e1.record(stream)
+            e1.synchronize()
+            best = max(best, 2 * a.numel() * 4 * reps / (e0.elapsed_time(e1) / 1e3) / 1e9)
+    del a, b
+    return best
+
+
 def fp32_flops_per_voxel_pulse(W: int) -> int:
     """Algorithmic FP32 work of the mixed kernel per voxel-pulse (FMA = 2 flops), counted
     from k_mixed.cu: per Fermat solve a (2W+1)^2 node scan at 17 flops per node, 4 facets x
@@ -815,6 +838,7 @@ def main():
 
     # ---------------- roofline of the dominant kernel (k_bp_mixed) ------------------
     peaks, peak_src = _peaks()
+    l2_gbs = l2_copy_gbs(torch, stream)
     clocks = clk.summary()
     sm_mhz = peaks.get("sm_max_mhz", 1965.0)
     fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12          # TFLOP/s, FMA = 2 flops
@@ -832,7 +856,9 @@ def main():
                         "note": "algorithmic count (both legs' rsqrt per scanned node); the warp's shared E-leg "
                                 "table executes about half of them"},
                 "gather": {"bytes_per_voxel_pulse": 16, "achieved_gbs": 16 * vp / (bp_avg_ms / 1e3) / 1e9,
-                           "hbm_peak_gbs": peaks.get("hbm_gbs"), "peak_source": peak_src},
+                           "hbm_peak_gbs": peaks.get("hbm_gbs"), "peak_source": peak_src,
+                           "l2_peak_gbs": l2_gbs,
+                           "l2_peak_source": "measured here: device copy of a 32 MiB buffer resident in L2"},
                 "fp32_flops_per_voxel_pulse": fp32_flops_per_voxel_pulse(W), "node_scan_half_width": W}
 
     # pulse compression (K1): HBM roofline on raw in + upsampled complex64 out

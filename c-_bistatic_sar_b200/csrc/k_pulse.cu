@@ -137,10 +137,12 @@ __device__ __forceinline__ unsigned brev_n(unsigned j, int logP) { return __brev
 // Reference spectrum: spec[j] = FFT(ref)[brev(j)] (conj when `conjugate` == 0 so that
 // the pulse kernel's conj(X) * spec is conj(X * G) for G = conj(H) or H).
 // ---------------------------------------------------------------------------------
+// rf_logP > 0: the spectrum of a register transform, stored in the order its third pass
+// reads (rf_spectrum_index); 0: bit-reversed order.
 template <typename R>
 __global__ void k_ref_spectrum(const double2* __restrict__ ref, int nref, int P, int logP,
                                const typename C2<R>::T* __restrict__ tw, int correlate,
-                               typename C2<R>::T* __restrict__ spec)
+                               typename C2<R>::T* __restrict__ spec, int rf_logP)
 {
     using V = typename C2<R>::T;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -153,7 +155,7 @@ __global__ void k_ref_spectrum(const double2* __restrict__ ref, int nref, int P,
     __syncthreads();
     fft_dif(x, P, logP, tw);
     for (int i = threadIdx.x; i < P; i += blockDim.x) {
-        V v = x[i];
+        V v = x[rf_logP ? rf_spectrum_index(rf_logP, i) : i];
         // correlation: G = conj(H) -> conj(G) = H ; convolution: G = H -> conj(G) = conj(H)
         spec[i] = correlate ? v : cconj(v);
     }
@@ -455,6 +457,42 @@ __device__ __forceinline__ void rf_dit4(float2 (&v)[16], int r, const float2* __
     }
 }
 
+// The same four stages on the second / fourth pass's blocks (STRIDE = B), twiddles from
+// the lane-ordered table (rf_twiddle_source): entry B (16 - 2d) + B (m mod d) + r.
+template <int L>
+__device__ __forceinline__ void rf_dif4b(float2 (&v)[16], int r, const float2* __restrict__ twb)
+{
+    constexpr int B = 16 << (L - 12);
+#pragma unroll
+    for (int d = 8; d >= 1; d >>= 1) {
+        asm volatile("" ::: "memory");
+#pragma unroll
+        for (int m = 0; m < 16; m++) {
+            if (m & d) continue;
+            const float2 a = v[m], b = v[m + d];
+            v[m] = cadd(a, b);
+            v[m + d] = cmul(csub(a, b), __ldg(twb + B * (16 - 2 * d) + B * (m & (d - 1)) + r));
+        }
+    }
+}
+
+template <int L>
+__device__ __forceinline__ void rf_dit4b(float2 (&v)[16], int r, const float2* __restrict__ twb)
+{
+    constexpr int B = 16 << (L - 12);
+#pragma unroll
+    for (int d = 1; d <= 8; d <<= 1) {
+        asm volatile("" ::: "memory");
+#pragma unroll
+        for (int m = 0; m < 16; m++) {
+            if (m & d) continue;
+            const float2 a = v[m], t = cmul(v[m + d], __ldg(twb + B * (16 - 2 * d) + B * (m & (d - 1)) + r));
+            v[m] = cadd(a, t);
+            v[m + d] = csub(a, t);
+        }
+    }
+}
+
 __device__ __forceinline__ float2 shfl_xor2(float2 a, int s)
 {
     a.x = __shfl_xor_sync(0xffffffffu, a.x, s);
@@ -499,7 +537,8 @@ template <int L> struct RfOcc { static constexpr int v = L == 14 ? 1 : 2; };
 template <int L>
 __global__ void __launch_bounds__((1 << L) / 16, RfOcc<L>::v)
     k_pulse_compress_rf(const double2* __restrict__ in, int ns, const float2* __restrict__ tw,
-                        const float2* __restrict__ spec, int n_keep, int factor, int out_kind,
+                        const float2* __restrict__ twb, const float2* __restrict__ spec, int n_keep, int factor,
+                        int out_kind,
                         double2* __restrict__ out64, float2* __restrict__ out32, __half2* __restrict__ out16,
                         float* __restrict__ scale16)
 {
@@ -529,7 +568,7 @@ __global__ void __launch_bounds__((1 << L) / 16, RfOcc<L>::v)
     // pass 2
     const int o2 = t % B, b2 = (t / B) * T + o2;
     rf_load<L, B>(x, v, b2);
-    rf_dif4<L, B>(v, o2, tw);
+    rf_dif4b<L>(v, o2, twb);
     rf_store<L, B>(x, v, b2);
     __syncthreads();
     // pass 3: last forward stages, matched filter, first inverse stages
@@ -542,7 +581,7 @@ __global__ void __launch_bounds__((1 << L) / 16, RfOcc<L>::v)
     for (int h = 0; h < 2; h++) {
         asm volatile("" ::: "memory");
 #pragma unroll
-        for (int m = 8 * h; m < 8 * h + 8; m++) v[m] = cmul(cconj(v[m]), __ldg(spec + b3 + TB * m));
+        for (int m = 8 * h; m < 8 * h + 8; m++) v[m] = cmul(cconj(v[m]), __ldg(spec + T * m + t));
     }
 #pragma unroll
     for (int s = 1; s < TB; s <<= 1) rf_dit_lanes<L>(v, sub, s, tw);
@@ -551,7 +590,7 @@ __global__ void __launch_bounds__((1 << L) / 16, RfOcc<L>::v)
     __syncthreads();
     // passes 2 and 1 of the inverse transform, then conj / P
     rf_load<L, B>(x, v, b2);
-    rf_dit4<L, B>(v, o2, tw);
+    rf_dit4b<L>(v, o2, twb);
     rf_store<L, B>(x, v, b2);
     __syncthreads();
     rf_load<L, T>(x, v, t);
@@ -966,12 +1005,13 @@ cudaError_t launch_ref_spectrum(const double2* ref, int nref, int P, int logP, c
         size_t sm = fft_smem_bytes<double>(P);
         cudaFuncSetAttribute(k_ref_spectrum<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         k_ref_spectrum<double><<<1, fft_threads(P), sm, st>>>(ref, nref, P, logP, (const double2*)tw, correlate,
-                                                            (double2*)spec);
+                                                            (double2*)spec, 0);
     } else {
         size_t sm = fft_smem_bytes<float>(P);
         cudaFuncSetAttribute(k_ref_spectrum<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        const int rf_logP = (rf_length(4, logP) && P == (1 << logP)) ? logP : 0;
         k_ref_spectrum<float><<<1, fft_threads(P), sm, st>>>(ref, nref, P, logP, (const float2*)tw, correlate,
-                                                           (float2*)spec);
+                                                           (float2*)spec, rf_logP);
     }
     return cudaGetLastError();
 }
@@ -983,17 +1023,19 @@ template <int L> static cudaError_t launch_pulse_rf(const PulseArgs& a, cudaStre
     // 60 % of the unified memory as shared memory holds two CTAs' pulses; the rest stays
     // L1 for the twiddles, the reference spectrum and register spills
     cudaFuncSetAttribute(k_pulse_compress_rf<L>, cudaFuncAttributePreferredSharedMemoryCarveout, 60);
+    if (!a.tw_rf) return cudaErrorInvalidValue;
     k_pulse_compress_rf<L><<<(unsigned)a.batch, (1 << L) / 16, sm, st>>>(
-        a.in, a.ns, (const float2*)a.tw, (const float2*)a.spec, a.n_keep, a.factor, a.out_kind, a.out64, a.out32,
-        a.out16, a.scale16);
+        a.in, a.ns, (const float2*)a.tw, (const float2*)a.tw_rf, (const float2*)a.spec, a.n_keep, a.factor,
+        a.out_kind, a.out64, a.out32, a.out16, a.scale16);
     return cudaGetLastError();
 }
 
 cudaError_t launch_pulse_compress(const PulseArgs& a, cudaStream_t st)
 {
     // FP32 transforms of 4096..16384 points into FP32 storage (or none): registers
-    if (a.real_bytes == 4 && (a.factor <= 0 || a.out_kind != 0) && a.logP >= 12 && a.logP <= 14 &&
-        a.P == (1 << a.logP)) {
+    if (rf_length(a.real_bytes, a.logP) && a.P == (1 << a.logP)) {
+        // the spectrum of these lengths is stored in the register transforms' order
+        if (a.factor > 0 && a.out_kind == 0) return cudaErrorInvalidValue;
         if (a.logP == 12) return launch_pulse_rf<12>(a, st);
         if (a.logP == 13) return launch_pulse_rf<13>(a, st);
         return launch_pulse_rf<14>(a, st);

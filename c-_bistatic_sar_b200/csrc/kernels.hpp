@@ -18,7 +18,10 @@ struct PulseArgs {
     int ns;
     int P, logP;         // padded FFT length
     const void* tw;      // P/2 twiddles, real_bytes precision
-    const void* spec;    // P reference-spectrum entries, bit-reversed order
+    const void* tw_rf;   // FP32 register transforms (4096..16384 points): the twiddles of their
+                         // second pass in lane order (rf_twiddle_count(P) entries, rf_twiddles)
+    const void* spec;    // P reference-spectrum entries, bit-reversed order (FP32 register
+                         // transforms: in the order their third pass reads, rf_spectrum_index)
     int real_bytes;      // 8: FP64 transform, 4: FP32 transform
     int n_keep;          // compressed samples kept per pulse
     int factor;          // 0: keep compressed (complex128 -> out64); >0 upsample
@@ -31,6 +34,32 @@ struct PulseArgs {
 
 cudaError_t launch_ref_spectrum(const double2* ref, int nref, int P, int logP, const void* tw, int correlate,
                                 void* spec, int real_bytes, cudaStream_t st);
+
+// FP32 pulse compression of P = 2^L points, 12 <= L <= 14, runs as register transforms
+// (k_pulse_compress_rf).  A P-point transform there is 16 elements a thread over T = P/16
+// threads in five passes; the second (and fourth) pass works on blocks of B = 16 TB
+// elements, TB = 2^(L-12), and the third on groups of TB.
+inline bool rf_length(int real_bytes, int logP) { return real_bytes == 4 && logP >= 12 && logP <= 14; }
+// Twiddles of the second / fourth pass in the order the lanes read them: for the stage of
+// span d (8, 4, 2, 1), entry B (16 - 2d) + B k + r holds twiddle (r + B k) P / (2 B d),
+// k < d, r < B; 15 B entries.
+inline int64_t rf_twiddle_count(int logP) { return 15LL * (16LL << (logP - 12)); }
+inline int64_t rf_twiddle_source(int logP, int64_t e)
+{
+    const int64_t P = 1LL << logP, B = 16LL << (logP - 12);
+    const int64_t blk = e / B, r = e % B;                 // blk in [0, 15): stage and k
+    const int64_t d = blk < 8 ? 8 : (blk < 12 ? 4 : (blk < 14 ? 2 : 1));
+    const int64_t k = blk - (16 - 2 * d);
+    return (r + B * k) * (P / (2 * B * d));
+}
+// Spectrum index that thread t reads for its element m in the third pass, stored at
+// m T + t: the element of group t / TB at offset t mod TB + TB m.
+inline __host__ __device__ int rf_spectrum_index(int logP, int o)
+{
+    const int T = 1 << (logP - 4), TB = 1 << (logP - 12), B = 16 * TB;
+    const int m = o / T, t = o % T;
+    return (t / TB) * B + t % TB + TB * m;
+}
 cudaError_t launch_pulse_compress(const PulseArgs& a, cudaStream_t st);
 // longest transform the FFT launchers take (a cluster of up to 8 CTAs)
 int64_t fft_max_len(int real_bytes);

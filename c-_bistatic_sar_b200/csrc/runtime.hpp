@@ -85,7 +85,7 @@ struct bsar_ctx {
     std::mutex mu;
     uint64_t next_scene = 1;
     std::map<uint64_t, std::unique_ptr<struct Scene>> scenes;
-    std::map<std::pair<int64_t, int>, std::unique_ptr<DevBuf>> twiddles;   // (P, real bytes)
+    std::map<std::pair<int64_t, int>, std::unique_ptr<DevBuf>> twiddles;   // (P, real bytes; -4: rf_twiddles)
     // cached grid axes for the asynchronous entry point
     std::vector<double> grid_host;
     std::unique_ptr<DevBuf> grid_dev;
@@ -398,6 +398,29 @@ inline const void* twiddles(bsar_ctx* ctx, int64_t P, int real_bytes)
     return p;
 }
 
+// The FP32 register transforms' second-pass twiddles in lane order (rf_twiddle_source):
+// the same FP32 values as twiddles(ctx, P, 4), rearranged.
+inline const void* rf_twiddles(bsar_ctx* ctx, int64_t P)
+{
+    const int logP = ilog2(P);
+    auto key = std::make_pair(P, -4);
+    auto it = ctx->twiddles.find(key);
+    if (it != ctx->twiddles.end()) return it->second->p;
+    const int64_t n = rf_twiddle_count(logP);
+    std::vector<float> w(2 * n);
+    for (int64_t e = 0; e < n; e++) {
+        const int64_t k = rf_twiddle_source(logP, e);
+        double a = -2.0 * kPi * (double)k / (double)P;
+        w[2 * e] = (float)std::cos(a);
+        w[2 * e + 1] = (float)std::sin(a);
+    }
+    auto b = dev_upload(ctx, w.data(), sizeof(float) * w.size());
+    sync(ctx);
+    const void* p = b->p;
+    ctx->twiddles[key] = std::move(b);
+    return p;
+}
+
 // longest FFT: one CTA up to 8192 (FP64) / 16384 (FP32) points, a cluster of up to 8 CTAs beyond
 inline int64_t max_fft_len(int real_bytes) { return fft_max_len(real_bytes); }
 
@@ -523,6 +546,7 @@ inline void compress_scene(bsar_ctx* ctx, Scene* s, int precision)
         fail(BSAR_ERR_UNSUPPORTED, "pulse length %lld exceeds the longest FFT (%lld for this precision)",
              (long long)s->ns, (long long)max_fft_len(a.real_bytes));
     a.tw = twiddles(ctx, a.P, a.real_bytes);
+    a.tw_rf = rf_length(a.real_bytes, a.logP) ? rf_twiddles(ctx, a.P) : nullptr;
     std::unique_ptr<DevBuf>& spec = s->spec[precision];
     if (!spec) {
         // the reference's spectrum once per scene and precision (the reference recomputes
