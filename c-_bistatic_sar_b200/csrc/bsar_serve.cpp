@@ -113,9 +113,11 @@ struct bsar_server {
     bsar_ctx* ctx = nullptr;
     bsar_server_opts opts{};
     uint64_t budget = 0, reserved = 0;
-    std::thread worker;
+    std::thread worker;                             // builds, launches and retires batches
+    std::thread io_thread;                          // admits requests, releases their buffers
     std::mutex mu;
-    std::condition_variable cv_work, cv_done;
+    std::condition_variable cv_work, cv_done, cv_io;
+    std::vector<Req*> to_free;                      // finished requests whose buffers await release
     bool stop = false;
     uint64_t next_id = 1;
     std::deque<Req*> pending;
@@ -128,7 +130,8 @@ struct bsar_server {
     Clock::time_point t_last_batch_done = Clock::now();
     double batch_busy_s = 0.0;                      // time with a batch on the device
     uint64_t batch_seq = 0;
-    cudaStream_t io = nullptr;
+    cudaStream_t io = nullptr;                      // admission and buffer release
+    cudaStream_t ret = nullptr;                     // image read-back of finished requests
     int grid_ctas = 0, max_tiles = 0;
     // statistics
     std::vector<double> latencies;
@@ -164,7 +167,9 @@ template <typename F> void with_ctx(bsar_server* s, cudaStream_t st, bool pooled
     s->ctx->use_pool = saved_pool;
 }
 
-void finish(bsar_server* s, Req* r, bsar_status st, const std::string& err)
+// Completes a request (server lock held).  keep_reserved: its device buffers are not
+// released yet, so its share of the budget stays reserved until the I/O thread frees them.
+void finish(bsar_server* s, Req* r, bsar_status st, const std::string& err, bool keep_reserved = false)
 {
     r->status = st;
     r->error = err;
@@ -172,8 +177,10 @@ void finish(bsar_server* s, Req* r, bsar_status st, const std::string& err)
     r->t_done = Clock::now();
     if (r->slot >= 0) s->slot_used[r->slot] = false;
     r->slot = -1;
-    s->reserved -= r->reserved;
-    r->reserved = 0;
+    if (!keep_reserved) {
+        s->reserved -= r->reserved;
+        r->reserved = 0;
+    }
     if (st == BSAR_OK) {
         s->completed++;
         s->vp_done += r->voxel_pulses;
@@ -195,7 +202,7 @@ void release(bsar_server* s, Req* r)
     });
 }
 
-// Admission of one request (worker thread, server lock NOT held): scene upload or
+// Admission of one request (I/O thread, server lock NOT held): scene upload or
 // synthesis, pulse compression + upsampling, anchors, device image.
 void admit(bsar_server* s, Req* r)
 {
@@ -204,18 +211,24 @@ void admit(bsar_server* s, Req* r)
         bsar_scene_desc d = r->desc;
         const bool synth = d.samples == nullptr;
         r->scene = make_scene(ctx, d, !synth);
-        if (synth) synthesize_samples(ctx, r->scene.get(), r->spos.data(), r->samp.data(), r->n_scat, r->snr_db, r->seed);
         check_newton_dem(r->scene->dem.view);
         if (r->scene->dem.view.empty || r->scene->dem.view.nx < 2 || r->scene->dem.view.ny < 2)
             fail(BSAR_ERR_UNSUPPORTED, "the mixed forms need a DEM of at least 2 x 2 nodes");
-        compress_scene(ctx, r->scene.get(), r->opts.precision);
-        sync(ctx);
-        r->scene->samples.reset();        // only the upsampled pulses are needed from here
+        // every upload from pageable memory before the first kernel (such a copy first
+        // drains the stream, whose kernels wait for SM slots behind the running batch), so
+        // the admission waits on the device once, for the anchors below
         std::vector<double> ax;
         ax.insert(ax.end(), r->gx.begin(), r->gx.end());
         ax.insert(ax.end(), r->gy.begin(), r->gy.end());
         ax.insert(ax.end(), r->gz.begin(), r->gz.end());
         r->axes = dev_upload(ctx, ax.data(), sizeof(double) * ax.size());
+        stage_reference(ctx, r->scene.get());
+        if (synth)
+            synthesize_samples(ctx, r->scene.get(), r->spos.data(), r->samp.data(), r->n_scat, r->snr_db, r->seed, 0,
+                               false);
+        compress_scene(ctx, r->scene.get(), r->opts.precision, false);
+        r->scene->samples.reset();        // only the upsampled pulses are needed from here (freed in stream order)
+        r->scene->reference_dev.reset();
         const int64_t nv = r->grid.nx * r->grid.ny * r->grid.nz;
         r->image = dev_alloc(ctx, sizeof(double2) * nv);
         Scene* sc = r->scene.get();
@@ -382,11 +395,12 @@ void launch_batch(bsar_server* s, ServeBatch& bt, int W, int n)
     s->tiles += n;
 }
 
-// Admits the oldest pending request if budget and slots allow (server lock held on entry
-// and exit; released around the device work).  Returns true if it took a request.
+// Admits the oldest pending request if budget and slots allow (I/O thread; server lock
+// held on entry and exit, released around the device work).  Returns true if it took a
+// request.
 bool admit_one(bsar_server* s, std::unique_lock<std::mutex>& lk)
 {
-    if (s->pending.empty() || s->stop) return false;
+    if (s->pending.empty() || s->stop || !s->fatal.empty()) return false;
     Req* r = s->pending.front();
     const uint64_t need = estimate_bytes(*r);
     int slot = -1;
@@ -420,12 +434,12 @@ bool admit_one(bsar_server* s, std::unique_lock<std::mutex>& lk)
     }
     if (st != BSAR_OK) release(s, r);
     lk.lock();
-    if (st == BSAR_OK && r->cancelled) {     // cancelled while being admitted
-        lk.unlock();
+    if (st == BSAR_OK && (r->cancelled || !s->fatal.empty())) {   // cancelled, or the server stopped,
+        lk.unlock();                                                // while it was being admitted
         release(s, r);
         lk.lock();
-        st = BSAR_ERR_CANCELLED;
-        err = "cancelled";
+        st = r->cancelled ? BSAR_ERR_CANCELLED : s->fatal_status;
+        err = r->cancelled ? "cancelled" : s->fatal;
     }
     if (st == BSAR_OK) {
         r->state = St::Active;
@@ -439,8 +453,8 @@ bool admit_one(bsar_server* s, std::unique_lock<std::mutex>& lk)
     return true;
 }
 
-// Waits (bounded) for batch `bt`, admitting pending requests while it runs.  Lock held
-// on entry and exit.  Returns an empty string, or why the batch failed.
+// Waits (bounded) for batch `bt`.  Lock held on entry and exit, released while it polls.
+// Returns an empty string, or why the batch failed.
 std::string wait_batch(bsar_server* s, ServeBatch& bt, std::unique_lock<std::mutex>& lk)
 {
     const auto t0 = Clock::now();
@@ -452,45 +466,74 @@ std::string wait_batch(bsar_server* s, ServeBatch& bt, std::unique_lock<std::mut
             s->fatal_status = BSAR_ERR_TIMEOUT;
             return "a batch did not finish within its time limit";
         }
-        if (!admit_one(s, lk)) {
-            lk.unlock();
-            std::this_thread::sleep_for(std::chrono::microseconds(50));
-            lk.lock();
-        }
+        lk.unlock();
+        std::this_thread::sleep_for(std::chrono::microseconds(50));
+        lk.lock();
     }
 }
 
+// Completes the admitted requests that need no more work (worker thread; server lock held
+// on entry and exit): each image is read back on the server's own stream, without the
+// context lock, so a running admission does not hold it up; the request completes at
+// once and its device buffers go to the I/O thread for release.
 void retire_finished(bsar_server* s, std::unique_lock<std::mutex>& lk)
 {
     std::vector<Req*> done;
     for (Req* r : s->active)
         if (r->done_tiles >= r->ntiles) done.push_back(r);
-    for (Req* r : done) {
-        s->active.erase(std::find(s->active.begin(), s->active.end(), r));
-        lk.unlock();
-        bsar_status st = BSAR_OK;
-        std::string err;
+    if (done.empty()) return;
+    for (Req* r : done) s->active.erase(std::find(s->active.begin(), s->active.end(), r));
+    lk.unlock();
+    std::vector<std::pair<bsar_status, std::string>> out(done.size(), {BSAR_OK, std::string()});
+    for (size_t k = 0; k < done.size(); k++) {
+        Req* r = done[k];
         if (r->cancelled) {
-            st = BSAR_ERR_CANCELLED;
-            err = "cancelled";
-        } else {
-            try {
-                with_ctx(s, s->io, true, [&] {
-                    cuda_check(cudaMemcpyAsync(r->image_out, r->image->p, r->image->bytes, cudaMemcpyDeviceToHost,
-                                               s->io),
-                               "image d2h");
-                    sync(s->ctx);
-                });
-            } catch (const Error& e) {
-                st = e.status;
-                err = e.msg;
-            }
+            out[k] = {BSAR_ERR_CANCELLED, "cancelled"};
+            continue;
         }
-        release(s, r);
-        lk.lock();
-        finish(s, r, st, err);
+        cudaError_t e = cudaMemcpyAsync(r->image_out, r->image->p, r->image->bytes, cudaMemcpyDeviceToHost, s->ret);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s->ret);
+        if (e != cudaSuccess) out[k] = {BSAR_ERR_CUDA, std::string("image d2h: ") + cudaGetErrorString(e)};
     }
-    if (!done.empty()) s->cv_done.notify_all();
+    lk.lock();
+    for (size_t k = 0; k < done.size(); k++) {
+        finish(s, done[k], out[k].first, out[k].second, true);
+        s->to_free.push_back(done[k]);
+    }
+    s->cv_done.notify_all();
+    s->cv_io.notify_all();
+}
+
+// Releases the device buffers of finished requests and returns their budget (I/O thread;
+// server lock held on entry and exit).  Returns true if there were any.
+bool free_finished(bsar_server* s, std::unique_lock<std::mutex>& lk)
+{
+    if (s->to_free.empty()) return false;
+    std::vector<Req*> v;
+    v.swap(s->to_free);
+    lk.unlock();
+    for (Req* r : v) release(s, r);
+    lk.lock();
+    for (Req* r : v) {
+        s->reserved -= r->reserved;
+        r->reserved = 0;
+    }
+    return true;
+}
+
+// The I/O thread: releases finished requests' buffers first (they return budget), then
+// admits the oldest pending request; admission's device work waits for SM slots behind
+// the running batch, and the worker keeps launching batches meanwhile.
+void io_main(bsar_server* s)
+{
+    cudaSetDevice(s->ctx->device);
+    std::unique_lock<std::mutex> lk(s->mu);
+    while (!s->stop) {
+        const bool freed = free_finished(s, lk);
+        const bool took = admit_one(s, lk);
+        if (took) s->cv_work.notify_all();
+        if (!freed && !took) s->cv_io.wait_for(lk, std::chrono::milliseconds(2));
+    }
 }
 
 void worker_main(bsar_server* s)
@@ -504,7 +547,9 @@ void worker_main(bsar_server* s)
                 if (bt.inflight) continue;
                 int W = 0;
                 const int n = build_batch(s, bt, &W);
-                if (n > 0) with_ctx(s, bt.st, false, [&] { launch_batch(s, bt, W, n); });
+                // no context lock: the launch touches only the server's own buffers and
+                // streams, so it does not wait for an admission that holds the context
+                if (n > 0) launch_batch(s, bt, W, n);
             }
         } catch (const Error& e) {
             s->fatal = e.msg;
@@ -515,12 +560,12 @@ void worker_main(bsar_server* s)
             if (bt.inflight && (!old || bt.seq < old->seq)) old = &bt;
         if (!old) {
             // nothing on the device: retire what needs no more work (cancelled requests),
-            // admit, or sleep until work arrives
+            // or sleep until the I/O thread admits work
             retire_finished(s, lk);
-            if (!admit_one(s, lk)) s->cv_work.wait_for(lk, std::chrono::milliseconds(2));
+            s->cv_work.wait_for(lk, std::chrono::milliseconds(2));
             continue;
         }
-        // 2. wait for the older batch, admitting meanwhile
+        // 2. wait for the older batch (the I/O thread admits meanwhile)
         std::string err = wait_batch(s, *old, lk);
         if (!err.empty()) {
             s->fatal = err;
@@ -530,7 +575,7 @@ void worker_main(bsar_server* s)
         // a bounded device wait that ran out: drain the other batch, fail both batches' requests
         std::string serr;
         try {
-            with_ctx(s, old->st, false, [&] { check_device_status(s->ctx); });
+            check_device_status(s->ctx);     // synchronous copies of the context's status word
         } catch (const Error& e) {
             serr = e.msg;
         }
@@ -637,6 +682,7 @@ bsar_status bsar_server_create(bsar_ctx* ctx, const bsar_server_opts* opts, bsar
         int least = 0, greatest = 0;
         cuda_check(cudaDeviceGetStreamPriorityRange(&least, &greatest), "stream priorities");
         cuda_check(cudaStreamCreateWithPriority(&s->io, cudaStreamNonBlocking, greatest), "stream");
+        cuda_check(cudaStreamCreateWithPriority(&s->ret, cudaStreamNonBlocking, greatest), "stream");
         for (ServeBatch& bt : s->batch) {
             cuda_check(cudaStreamCreateWithPriority(&bt.st, cudaStreamNonBlocking, least), "stream");
             cuda_check(cudaEventCreateWithFlags(&bt.ev, cudaEventDisableTiming), "event");
@@ -662,6 +708,7 @@ bsar_status bsar_server_create(bsar_ctx* ctx, const bsar_server_opts* opts, bsar
     }
     bsar_server* raw = s.release();
     raw->worker = std::thread(worker_main, raw);
+    raw->io_thread = std::thread(io_main, raw);
     *out = raw;
     return BSAR_OK;
 }
@@ -723,7 +770,7 @@ bsar_status bsar_server_submit(bsar_server* s, const bsar_request* q, bsar_reque
     *out = r->id;
     s->pending.push_back(r.get());
     s->reqs[r->id] = std::move(r);
-    s->cv_work.notify_all();
+    s->cv_io.notify_all();
     return BSAR_OK;
 }
 
@@ -785,10 +832,11 @@ bsar_status bsar_server_cancel(bsar_server* s, bsar_request_id id)
         s->cv_done.notify_all();
         return BSAR_OK;
     }
-    // admitted (or being admitted): no further work items; the worker releases it when the
+    // admitted (or being admitted): no further work items; the worker completes it when the
     // items already on the device are done
     if (r->state == St::Active) r->ntiles = r->next_tile;
     s->cv_work.notify_all();
+    s->cv_io.notify_all();
     return BSAR_OK;
 }
 
@@ -825,8 +873,10 @@ void bsar_server_destroy(bsar_server* s)
         std::lock_guard<std::mutex> lk(s->mu);
         s->stop = true;
         s->cv_work.notify_all();
+        s->cv_io.notify_all();
     }
     if (s->worker.joinable()) s->worker.join();
+    if (s->io_thread.joinable()) s->io_thread.join();
     {
         std::lock_guard<std::mutex> lk(s->ctx->mu);
         cudaSetDevice(s->ctx->device);
@@ -859,6 +909,10 @@ void bsar_server_destroy(bsar_server* s)
             if (bt.st) cudaStreamDestroy(bt.st);
         }
         if (s->io) cudaStreamDestroy(s->io);
+        if (s->ret) {
+            cudaStreamSynchronize(s->ret);
+            cudaStreamDestroy(s->ret);
+        }
     }
     delete s;
 }

@@ -440,6 +440,7 @@ struct Scene {
     double n1 = 1, n2 = 1, c = 3e8, fc = 1e9, fs = 1e9, f0 = 0, f1 = 0, T = 0;
     std::unique_ptr<DevBuf> tx, rx, samples;
     std::vector<double> reference;     // matched-filter reference (Ns complex), RAW scenes
+    std::unique_ptr<DevBuf> reference_dev;   // the reference on the device (stage_reference)
     RcBuf rc[3];                       // per bsar_precision
     std::unique_ptr<DevBuf> spec[3];   // matched-filter spectrum per precision (bit-reversed)
     // mixed-form anchors (per grid centre and node-scan width)
@@ -511,7 +512,23 @@ inline std::vector<double> matched_reference(double f0, double f1, double T, dou
     return ref;
 }
 
-inline void compress_scene(bsar_ctx* ctx, Scene* s, int precision)
+// Copies the scene's matched-filter reference to the device now, so that a later
+// compress_scene enqueues no upload from pageable memory (which would first drain the
+// stream).
+inline void stage_reference(bsar_ctx* ctx, Scene* s)
+{
+    if (!s->reference.empty() && !s->reference_dev)
+        s->reference_dev = dev_upload(ctx, s->reference.data(), sizeof(double) * s->reference.size());
+}
+
+// Device buffers come from the stream-ordered pool: a temporary released at the end of an
+// enqueuing function is freed in stream order, so the function need not wait for its
+// kernels.
+inline bool stream_ordered(const bsar_ctx* ctx) { return ctx->use_pool && ctx->pool; }
+
+// Enqueues the compression; with wait = true (or without pooled buffers) it first waits
+// for the reference spectrum it had to build.
+inline void compress_scene(bsar_ctx* ctx, Scene* s, int precision, bool wait = true)
 {
     RcBuf& rb = s->rc[precision];
     const int64_t nr = s->nr;
@@ -552,12 +569,13 @@ inline void compress_scene(bsar_ctx* ctx, Scene* s, int precision)
         // the reference's spectrum once per scene and precision (the reference recomputes
         // it for every pulse, src/fft_utils.cpp:81-82)
         spec = dev_alloc(ctx, (size_t)a.P * (a.real_bytes == 8 ? sizeof(double2) : sizeof(float2)));
-        const std::vector<double>& ref = s->reference;
-        auto dref = dev_upload(ctx, ref.data(), sizeof(double) * ref.size());
+        std::unique_ptr<DevBuf> tmp;
+        if (!s->reference_dev) tmp = dev_upload(ctx, s->reference.data(), sizeof(double) * s->reference.size());
+        const DevBuf* dref = s->reference_dev ? s->reference_dev.get() : tmp.get();
         launched(ctx, launch_ref_spectrum(dref->as<double2>(), (int)s->ns, a.P, a.logP, a.tw, 1, spec->p,
                                           a.real_bytes, ctx->stream),
                  "reference spectrum");
-        sync(ctx);
+        if (wait || !stream_ordered(ctx)) sync(ctx);
     }
     a.spec = spec->p;
     launched(ctx, launch_pulse_compress(a, ctx->stream), "pulse compression");
@@ -622,8 +640,10 @@ inline std::unique_ptr<Scene> make_scene(bsar_ctx* ctx, const bsar_scene_desc& s
 
 
 // Echo synthesis into a scene's raw pulses (bsar_scene_synthesize), on ctx->stream.
+// wait = false (pooled buffers only): return once the work is enqueued; the scatterer
+// arrays are read before the call returns either way.
 inline void synthesize_samples(bsar_ctx* ctx, Scene* sc, const double* scat_pos, const double* scat_amp, int64_t n_scat,
-                               double snr_db, uint64_t seed, int flags = 0)
+                               double snr_db, uint64_t seed, int flags = 0, bool wait = true)
 {
     check_newton_dem(sc->dem.view);
     const int W = search_nodes(sc->dem.view, 0.0);
@@ -645,7 +665,7 @@ inline void synthesize_samples(bsar_ctx* ctx, Scene* sc, const double* scat_pos,
                                     (flags & BSAR_SYNTH_REFERENCE_BINS) ? 1 : 0, tau->as<double>(),
                                     car->as<double2>(), sc->samples->as<double2>(), ctx->stream),
              "echo synthesis");
-    sync(ctx);   // the work buffers are released on return
+    if (wait || !stream_ordered(ctx)) sync(ctx);   // the work buffers are released on return
 }
 
 // Per-pulse anchors of the mixed form at the grid centre (FP64 reference path, reduced

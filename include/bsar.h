@@ -349,12 +349,13 @@ bsar_status bsar_dem_load_esri(const char* path, int64_t* nx, int64_t* ny, doubl
 
 /* ---------------------------------------------------------------------------------
  * Serving: image-formation requests of different grids, pulse counts and DEMs are
- * admitted as they arrive (FIFO) against an HBM budget; each admitted request's scene
- * stays resident while its voxel tiles (128 voxels each) are packed with other requests'
- * tiles into one persistent mixed-kernel launch per batch (optionally a replayed CUDA
- * graph), earliest deadline first (arrival plus twice the request's own service time at
- * the server's recent throughput).  Requests that arrive while others run join the next batch.  A voxel's result
- * does not depend on what else shares its batch.
+ * admitted as they arrive (FIFO) against an HBM budget, by a thread of their own while
+ * the batches run; each admitted request's scene stays resident while its voxel tiles
+ * (128 voxels each) are packed with other requests' tiles into one persistent
+ * mixed-kernel launch per batch (optionally a replayed CUDA graph), earliest deadline
+ * first (arrival plus twice the request's own service time at the server's recent
+ * throughput).  Requests that arrive while others run join the next batch.  A voxel's
+ * result does not depend on what else shares its batch.
  * ------------------------------------------------------------------------------- */
 typedef struct bsar_server bsar_server;
 typedef uint64_t bsar_request_id;
