@@ -452,11 +452,13 @@ __device__ __forceinline__ void scan_pruned(const MixedCtx& m, const AirTable& A
     const float ay2 = 2.0f * ay;
     const float yfirst = (float)(js - W) * m.stepy - gy;
     // height monotonicity over the window, from the DEM's lowest height (else nothing is
-    // pruned)
+    // pruned): d/dZ [a_z Z + |N - G|] = a_z + Z / |N - G| (Z above the voxel) is positive
+    // for every node only if the voxel lies below the DEM's lowest height (Z >= Zt > 0),
+    // and, for a_z < 0, Z^2 >= a_z^2 |N - G|^2 at the window's farthest corner
     const float Zt = m.zmin - gz;
     const float hx = fabsf(x0 - gx) + (float)W * m.stepx, hy = fabsf(y0 - gy) + (float)W * m.stepy;
     const bool bound_ok = sy2 > 1e-3f &&           // |a| = re: the bound needs the E leg's index below the G leg's
-                          (az >= 0.0f || (Zt > 0.0f && az * az * (hx * hx + hy * hy + Zt * Zt) <= Zt * Zt));
+                          Zt > 0.0f && (az >= 0.0f || az * az * (hx * hx + hy * hy + Zt * Zt) <= Zt * Zt);
     // seed: the previous pulse's best node, ranked with the scan's own arithmetic
     float thr_seed = INFINITY;
     {
