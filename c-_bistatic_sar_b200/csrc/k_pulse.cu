@@ -399,22 +399,44 @@ template <int L> __device__ __forceinline__ int swz(int e)
     return e ^ (((e >> (4 + lt)) & (15 >> lt)) << lt);
 }
 
+// swz(base + STRIDE m) for the bases the passes use, from one swizzle of the base: the
+// first and fifth pass (STRIDE = T, base = t) add T m above the swizzled bits; the second
+// and fourth (STRIDE = B, base = (t / B) T + t mod B) take m's low bits as the swizzle
+// key, a constant for each m; the third (STRIDE = TB, base = (t / TB) B + t mod TB) flips
+// m into the swizzled field.  One or no instruction per element instead of five.
+template <int L, int STRIDE> __device__ __forceinline__ int rf_sbase(int base)
+{
+    constexpr int B = 16 << (L - 12);
+    return STRIDE == B ? base : swz<L>(base);
+}
+
+template <int L, int STRIDE> __device__ __forceinline__ int rf_index(int sb, int m)
+{
+    constexpr int T = 1 << (L - 4), B = 16 << (L - 12), lt = L - 12;
+    static_assert(STRIDE == T || STRIDE == B || STRIDE == (1 << lt), "a pass stride");
+    if constexpr (STRIDE == T) return sb + T * m;
+    else if constexpr (STRIDE == B) return (sb ^ ((m & (15 >> lt)) << lt)) + B * m;
+    else return sb ^ (m << lt);
+}
+
 // The opaque copy of `base` makes each call compute its 16 addresses afresh, instead of
 // the compiler keeping a pass's addresses live until the inverse pass reuses them.
 template <int L, int STRIDE>
 __device__ __forceinline__ void rf_load(const float2* x, float2 (&v)[16], int base)
 {
     asm volatile("" : "+r"(base));
+    const int sb = rf_sbase<L, STRIDE>(base);
 #pragma unroll
-    for (int m = 0; m < 16; m++) v[m] = x[swz<L>(base + STRIDE * m)];
+    for (int m = 0; m < 16; m++) v[m] = x[rf_index<L, STRIDE>(sb, m)];
 }
 
 template <int L, int STRIDE>
 __device__ __forceinline__ void rf_store(float2* x, const float2 (&v)[16], int base)
 {
     asm volatile("" : "+r"(base));
+    const int sb = rf_sbase<L, STRIDE>(base);
 #pragma unroll
-    for (int m = 0; m < 16; m++) x[swz<L>(base + STRIDE * m)] = v[m];
+    for (int m = 0; m < 16; m++) x[rf_index<L, STRIDE>(sb, m)] = v[m];
 }
 
 // Four DIF stages (spans 8, 4, 2, 1 x STRIDE) on elements base + STRIDE m; r = base mod
