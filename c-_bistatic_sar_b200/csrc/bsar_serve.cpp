@@ -1,21 +1,25 @@
 // bsar_serve.cpp -- continuous-batching image-formation server (bsar_server_* of bsar.h).
 //
-// One worker thread per server owns the GPU work.  Two batch slots, each with its own
-// stream, pinned staging and device copies, keep up to two batches in flight:
+// Two threads per server.  The worker owns the batches: two batch slots, each with its
+// own stream, pinned staging and device copies, keep up to two batches in flight:
 //
 //   loop:
 //     fill every idle batch slot: a list of (request, work item) pairs -- a 128-voxel
 //       tile, or one pulse chunk of a tile for small grids -- of the admitted requests in
 //       earliest-deadline order (arrival + twice the request's own service time), most
-//       costly items first, launched as a replay of a
-//       captured CUDA graph (request records and tile list copied from pinned staging,
-//       work counter zeroed, persistent mixed kernel)
-//     wait for the older batch (bounded); while it runs, admit pending requests FIFO
-//       as the HBM budget and the in-flight slots allow (scene upload or on-device echo
-//       synthesis, pulse compression + upsampling, per-pulse anchors; `io` stream,
-//       stream-ordered allocations, so admission never waits for a batch)
-//     retire requests whose tiles are all done (image to the caller's buffer,
-//       resources released, latency recorded)
+//       costly items first, launched as a replay of a captured CUDA graph (request
+//       records and tile list copied from pinned staging, work counter zeroed,
+//       persistent mixed kernel); no context lock
+//     wait for the older batch (bounded)
+//     retire requests whose tiles are all done (image to the caller's buffer on the
+//       `ret` stream, latency recorded; the buffers go to the I/O thread)
+//
+// The I/O thread frees finished requests' buffers (which returns their budget) and admits
+// pending requests FIFO as the HBM budget and the in-flight slots allow: scene upload or
+// on-device echo synthesis, pulse compression + upsampling, per-pulse anchors, on the
+// high-priority `io` stream with stream-ordered allocations.  Every upload comes before
+// the first kernel, so an admission waits on the device once (the anchors' read-back),
+// and its kernels take SM slots as the running batch's CTAs free them.
 //
 // The second batch's CTAs take the SMs the first batch's tail leaves idle.  Work items
 // are the same 128-voxel groups (and pulse chunks) a one-request launch uses, so every
