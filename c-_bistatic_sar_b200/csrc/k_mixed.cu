@@ -139,18 +139,20 @@ __device__ __forceinline__ bool facet_step32(const Facet32& F, const float A[3],
     float hxx = g1 * (txx - a1x * a1x * iq1) + g2 * (txx - a2x * a2x * iq2);
     float hyy = g1 * (tyy - a1y * a1y * iq1) + g2 * (tyy - a2y * a2y * iq2);
     float hxy = g1 * (txy - a1x * a1y * iq1) + g2 * (txy - a2x * a2y * iq2) + (g1 * r1z + g2 * r2z) * zxy;
-    float igs = __frcp_rn(g1 + g2);
+    // approximate reciprocals (2 ulp): they set a Newton step's length, which the FP64
+    // final step corrects, so a correctly rounded one buys nothing
+    float igs = __fdividef(1.0f, g1 + g2);
     float su, sv;
     if (au) {
         su = 0.0f;
-        sv = (hyy > 0.0f) ? -gy * __frcp_rn(hyy) : -gy * igs;
+        sv = (hyy > 0.0f) ? -gy * __fdividef(1.0f, hyy) : -gy * igs;
     } else if (av) {
         sv = 0.0f;
-        su = (hxx > 0.0f) ? -gx * __frcp_rn(hxx) : -gx * igs;
+        su = (hxx > 0.0f) ? -gx * __fdividef(1.0f, hxx) : -gx * igs;
     } else {
         float det = hxx * hyy - hxy * hxy;
         if (det > 0.0f && hxx > 0.0f) {
-            float idet = __frcp_rn(det);
+            float idet = __fdividef(1.0f, det);
             su = -(hyy * gx - hxy * gy) * idet;
             sv = -(hxx * gy - hxy * gx) * idet;
         } else {
@@ -444,11 +446,14 @@ __device__ __forceinline__ void scan_pruned(const MixedCtx& m, const AirTable& A
     // tangent plane of the E leg at the start node N0
     const float2 n0 = row0[W * TBJ + W];
     const float x0 = (float)is * m.stepx, y0 = (float)js * m.stepy;
-    const float kk = re * re / n0.y;                    // re / |N0 - E|
+    // approximate divisions (2 ulp): the tangent plane and the parabola's vertex move by
+    // ~1e-7 relative, which changes the bound by far less than the threshold's margin
+    // (2e-4 m + 4e-6 |T|), so the skips stay exact
+    const float kk = __fdividef(re * re, n0.y);                    // re / |N0 - E|
     const float ax = (x0 - E[0]) * kk, ay = (y0 - E[1]) * kk, az = (n0.x - E[2]) * kk;
     const float K = n0.y + ax * (gx - x0) + ay * (gy - y0) + az * (gz - n0.x);
     const float sy2 = 1.0f - ay * ay;
-    const float yv_t = -ay / sy2;                       // vertex of the parabola: Y = t * yv_t
+    const float yv_t = __fdividef(-ay, sy2);                       // vertex of the parabola: Y = t * yv_t
     const float ay2 = 2.0f * ay;
     const float yfirst = (float)(js - W) * m.stepy - gy;
     // height monotonicity over the window, from the DEM's lowest height (else nothing is
@@ -737,7 +742,7 @@ __device__ __forceinline__ double solve_mixed(const DemView& d, const MixedCtx& 
     const float* E = g_is_b ? A32 : B32;
     const float* G = g_is_b ? B32 : A32;
     const float ng = g_is_b ? nb : na;
-    const float re = (g_is_b ? na : nb) / ng;
+    const float re = __fdividef(g_is_b ? na : nb, ng);
     AirTable AT{table_buf, 0, 0, false};
     if constexpr (TABLE && WT > 0)
         AT = build_air_table<TableRows<WT>::v>(m, T, table_buf, is, js, W, E[0], E[1], E[2], re);
