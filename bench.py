@@ -52,8 +52,8 @@ sys.path.insert(0, str(ROOT / "c-_bistatic_sar_b200"))
 METRIC = "BP voxel-pulses/s (Fermat incl.), mixed vs FP64 @<=1e-3 rel-L2; served p99 ms"
 # DRAM bytes (read + write) of one k_bp_mixed launch on the full medium scene: a one-pass
 # ncu capture of dram__bytes_read.sum + dram__bytes_write.sum of the headline command
-# (4.18 MB + 2.46 MB; the gathers hit L2, and the image leaves L2 after the kernel ends)
-TRAFFIC_BYTES = {2: 6.64e6}
+# (4.06 MB + 2.47 MB; the gathers hit L2, and the image leaves L2 after the kernel ends)
+TRAFFIC_BYTES = {2: 6.53e6}
 UNIT = "voxel-pulses/s"
 
 
